@@ -1,0 +1,438 @@
+#!/usr/bin/env python3
+"""Benchmark of the sm_100a SLEEK compress / decompress path.
+
+Metric (the reference's convention, sleek_single_compressor.cu:123 and
+memcpy.cu:128): GB/s of UNCOMPRESSED bytes, 1e9 bytes per GB.
+
+Workload (default): the float64 turbulence-like field of 256 x 384 x 384 values
+(301,989,888 bytes; seeded synthetic stand-in for the Miranda field), lossless
+and absolute error bounds 1e-2, 1e-4, 1e-6.  One step = compress + decompress
+of the field in each of the four modes (8 kernel launches, each preceded by a
+workspace clear).  Inputs (302 MB) are larger than the 126 MB L2, so no flush is
+needed between iterations.
+
+  value     whole-job GB/s: uncompressed bytes through all compress and
+            decompress passes of all ranks / max-over-ranks device time
+  e2e       same metric through the public C-ABI calls with host buffers:
+            per mode H2D of the input, compress, D2H of the stream, H2D of the
+            stream, decompress, D2H of the output, all inside the timed region
+  roofline  the dominant kernel's algorithmic bytes (uncompressed + stream
+            bytes per launch) / its mean CUDA-event duration, against the
+            measured HBM copy bandwidth in MEASURED_PEAKS.json
+  cpu_baseline  the reference's own OpenMP CPU codec (oracle/_ref), all host
+            threads, on the same field
+
+Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU (torchrun, one process per GPU): every rank runs an independent
+replica of the workload (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "compress/decompress GB/s (uncompressed bytes) vs D2D memcpy on 1 B200"
+MODES = [None, 1e-2, 1e-4, 1e-6]
+SHAPE = (256, 384, 384)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+# ---------------------------------------------------------------------------------
+# reference arm: the reference's own CPU codec on the host cores
+# ---------------------------------------------------------------------------------
+
+def cpu_reference_run(x: np.ndarray, repeats: int):
+    """Times the reference CPU codec (compress + decompress, every mode) on x."""
+    from oracle import oracle as O
+
+    if O.ref_cpu() is None:
+        return None, "port"
+    t_total = 0.0
+    nbytes = 0
+    for _ in range(repeats):
+        for eb in MODES:
+            t0 = time.perf_counter()
+            s = O.ref_encode(x, eb)
+            t1 = time.perf_counter()
+            O.ref_decode(s, x.dtype, eb)
+            t2 = time.perf_counter()
+            t_total += t2 - t0
+            nbytes += 2 * x.nbytes
+    return nbytes / t_total / 1e9, "reference"
+
+
+def cpu_port_run(x: np.ndarray, repeats: int):
+    from oracle import oracle as O
+
+    t_total = 0.0
+    nbytes = 0
+    for _ in range(repeats):
+        for eb in MODES:
+            t0 = time.perf_counter()
+            s = O.encode(x, eb)
+            O.decode(s, x.dtype, eb)
+            t_total += time.perf_counter() - t0
+            nbytes += 2 * x.nbytes
+    return nbytes / t_total / 1e9
+
+
+def cpu_baseline(x_host: np.ndarray, max_seconds: float = 20.0):
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    cores = int(os.environ["OMP_NUM_THREADS"])
+    t0 = time.perf_counter()
+    v, kind = cpu_reference_run(x_host, 1)
+    if v is None:
+        v = cpu_port_run(x_host, 1)
+        kind, cores = "port", 1
+    el = time.perf_counter() - t0
+    reps = max(1, min(5, int(max_seconds / max(el, 1e-3))))
+    if reps > 1:
+        v2 = cpu_reference_run(x_host, reps)[0] if kind == "reference" else cpu_port_run(x_host, reps)
+        v = v2
+    return {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+            "sample": f"full {x_host.nbytes} B field, compress+decompress x 4 modes, {reps + 1} passes"}
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from sleek_b200 import workloads
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    x = workloads.c1_turbulence(SHAPE, device=dev).cpu().numpy()
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_cpu() is not None else "port"
+    cores = int(os.environ["OMP_NUM_THREADS"]) if kind == "reference" else 1
+    run = (lambda r: cpu_reference_run(x, r)[0]) if kind == "reference" else (lambda r: cpu_port_run(x, r))
+    for _ in range(args.warmup):
+        run(1)
+    t0 = time.perf_counter()
+    steps_v = [run(1) for _ in range(args.steps)]
+    el = time.perf_counter() - t0
+    v = statistics.mean(steps_v)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * el / max(args.steps, 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args),
+        "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+                         "sample": f"full {x.nbytes} B field, compress+decompress x 4 modes per step"},
+        "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": "c1 f64 turbulence field 256x384x384 (301,989,888 B), lossless + eb 1e-2/1e-4/1e-6, "
+                        "compress+decompress per mode",
+            "global_batch": 8 * args.gpus, "seq_len": None, "parallelism": f"replicas{args.gpus}",
+            "l2": "inputs larger than L2 (302 MB > 126 MB), no flush"}
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    from sleek_b200 import _capi, api, workloads
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L = _capi.lib()
+    x = workloads.c1_turbulence(SHAPE, device=dev)
+    N = x.numel() * 8
+    cap = api.sleek_upper_bound_size(N)
+    st = torch.cuda.current_stream()
+    sh = st.cuda_stream
+    # persistent device buffers, one stream buffer per mode
+    enc = [torch.empty(cap, dtype=torch.uint8, device=dev) for _ in MODES]
+    esz = torch.zeros(len(MODES), dtype=torch.int64, device=dev)
+    dsz = torch.zeros(len(MODES), dtype=torch.int64, device=dev)
+    dec = torch.empty_like(x)
+    wsz = max(L.sleek_compress_workspace_size(N), L.sleek_decompress_workspace_size())
+    ws = torch.zeros(wsz, dtype=torch.uint8, device=dev)
+    ebi = [None if eb is None else api.sleek_error_bound(eb, np.float64).c_struct() for eb in MODES]
+
+    def launch_c(i):
+        if ebi[i] is None:
+            rc = L.sleek_compress_f64(x.data_ptr(), x.numel(), enc[i].data_ptr(), esz[i:].data_ptr(),
+                                      ws.data_ptr(), wsz, sh)
+        else:
+            rc = L.sleek_compress_lossy_f64(ebi[i], x.data_ptr(), x.numel(), enc[i].data_ptr(),
+                                            esz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+        _capi.check(rc, "compress")
+
+    def launch_d(i):
+        if ebi[i] is None:
+            rc = L.sleek_decompress_f64(enc[i].data_ptr(), cap, dec.data_ptr(), N, dsz[i:].data_ptr(),
+                                        ws.data_ptr(), wsz, sh)
+        else:
+            rc = L.sleek_decompress_lossy_f64(ebi[i], enc[i].data_ptr(), cap, dec.data_ptr(), N,
+                                              dsz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+        _capi.check(rc, "decompress")
+
+    # correctness gate before timing: every mode round-trips and sizes are sane
+    for i in range(len(MODES)):
+        launch_c(i)
+        launch_d(i)
+    torch.cuda.synchronize()
+    S = [int(v) for v in esz.cpu().tolist()]
+    assert all(s > 0 for s in S) and all(int(v) == N for v in dsz.cpu().tolist()), (S, dsz)
+
+    # ---- per-kernel CUDA-event timing (the roofline numbers) ------------------------
+    reps = 10
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(len(MODES) * reps)]
+    for i in range(len(MODES)):
+        launch_c(i)
+        launch_d(i)
+    torch.cuda.synchronize()
+    k = 0
+    for r in range(reps):
+        for i in range(len(MODES)):
+            e = ev[k]; k += 1
+            e[0].record(st); launch_c(i); e[1].record(st)
+            e[2].record(st); launch_d(i); e[3].record(st)
+    torch.cuda.synchronize()
+    tc = [0.0] * len(MODES)
+    td = [0.0] * len(MODES)
+    k = 0
+    for r in range(reps):
+        for i in range(len(MODES)):
+            e = ev[k]; k += 1
+            tc[i] += e[0].elapsed_time(e[1]) / reps
+            td[i] += e[2].elapsed_time(e[3]) / reps
+    # memcpy D2D baseline on the same bytes (memcpy.cu:121-129 convention)
+    mc = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(3):
+        dec.copy_(x)
+    mc[0].record(st)
+    for _ in range(reps):
+        dec.copy_(x)
+    mc[1].record(st)
+    torch.cuda.synchronize()
+    t_memcpy = mc[0].elapsed_time(mc[1]) / reps
+    memcpy_gbs = N / (t_memcpy * 1e-3) / 1e9
+
+    # ---- whole-step timing ------------------------------------------------------------
+    def step():
+        for i in range(len(MODES)):
+            launch_c(i)
+            launch_d(i)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0.record(st)
+    for _ in range(args.steps):
+        step()
+    t1.record(st)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.stop()
+    ms = t0.elapsed_time(t1)
+    ms_max = dist_max(ms, world)
+    bytes_per_step = 2 * N * len(MODES)
+    value = bytes_per_step * args.steps * world / (ms_max * 1e-3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers --------------------------------
+    hin = torch.empty(x.numel(), dtype=torch.float64, pin_memory=True)
+    hin.copy_(x.cpu())
+    hstream = [torch.empty(cap, dtype=torch.uint8, pin_memory=True) for _ in MODES]
+    hout = torch.empty(x.numel(), dtype=torch.float64, pin_memory=True)
+    d_in = torch.empty_like(x)
+    d_enc = [torch.empty(cap, dtype=torch.uint8, device=dev) for _ in MODES]
+    h2d = sum(N + s for s in S)
+    d2h = sum(s + N for s in S)
+
+    def e2e_step():
+        for i in range(len(MODES)):
+            d_in.copy_(hin, non_blocking=True)
+            if ebi[i] is None:
+                rc = L.sleek_compress_f64(d_in.data_ptr(), x.numel(), d_enc[i].data_ptr(), esz[i:].data_ptr(),
+                                          ws.data_ptr(), wsz, sh)
+            else:
+                rc = L.sleek_compress_lossy_f64(ebi[i], d_in.data_ptr(), x.numel(), d_enc[i].data_ptr(),
+                                                esz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+            _capi.check(rc)
+            hstream[i][: S[i]].copy_(d_enc[i][: S[i]], non_blocking=True)
+            d_enc[i][: S[i]].copy_(hstream[i][: S[i]], non_blocking=True)
+            if ebi[i] is None:
+                rc = L.sleek_decompress_f64(d_enc[i].data_ptr(), S[i], dec.data_ptr(), N, dsz[i:].data_ptr(),
+                                            ws.data_ptr(), wsz, sh)
+            else:
+                rc = L.sleek_decompress_lossy_f64(ebi[i], d_enc[i].data_ptr(), S[i], dec.data_ptr(), N,
+                                                  dsz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+            _capi.check(rc)
+            hout.copy_(dec, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = dist_max(e0.elapsed_time(e1), world)
+    e2e_value = bytes_per_step * args.e2e_steps * world / (e2e_ms * 1e-3) / 1e9
+    assert all(int(v) == N for v in dsz.cpu().tolist()), dsz
+
+    # ---- roofline of the dominant kernel ----------------------------------------------
+    peak, peak_kind = peaks()
+    t_enc = sum(tc)
+    t_dec = sum(td)
+    dom = "encode" if t_enc >= t_dec else "decode"
+    per = tc if dom == "encode" else td
+    alg_bytes = sum(N + s for s in S) / len(MODES)
+    t_launch = sum(per) / len(MODES)
+    achieved = alg_bytes / (t_launch * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args),
+        "compress_gbs": {str(m): round(N / (tc[i] * 1e-3) / 1e9, 1) for i, m in enumerate(MODES)},
+        "decompress_gbs": {str(m): round(N / (td[i] * 1e-3) / 1e9, 1) for i, m in enumerate(MODES)},
+        "ratio": {str(m): round(N / S[i], 4) for i, m in enumerate(MODES)},
+        "memcpy_d2d_gbs": round(memcpy_gbs, 1),
+        "frac_of_memcpy": {
+            "compress": round(len(MODES) * N / (t_enc * 1e-3) / 1e9 / memcpy_gbs, 3),
+            "decompress": round(len(MODES) * N / (t_dec * 1e-3) / 1e9 / memcpy_gbs, 3)},
+        "roofline": {"bound": "hbm", "kernel": f"k_{dom}<u64> (mean over the 4 modes)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "peak_kind": f"of {peak_kind}", "traffic": None},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 2 * len(MODES) * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,124 @@
+/*
+ * sleek_capi.h -- C ABI of the B200 (sm_100a) SLEEK compress / decompress path.
+ *
+ * Drop-in boundary for the reference's GPU API (include/sleek_lossless_gpu.h and
+ * include/sleek_lossy_gpu.h of SLEEK).  Plain pointers and sizes only; every entry
+ * point is asynchronous on the given CUDA stream (NULL = legacy default stream) and
+ * returns a status code for everything it can check on the host.  Errors found on
+ * the device (malformed stream, a look-back wait that exceeded its time limit)
+ * never trap: the kernel writes -status into the size output (*d_encsize or
+ * *d_decsize), and the status is also readable with sleek_workspace_status().
+ *
+ * The compressed byte stream is SLEEK's own (8-byte insize, uint16 size per 16 KB
+ * chunk, byte-packed chunk payloads) and is bit-identical to the reference's CPU
+ * and GPU output for the same input and error bound.
+ *
+ * Pointers: device inputs/outputs must be aligned to their element size (4 for
+ * float, 8 for double); the stream buffer must be 8-byte aligned.  16-byte
+ * aligned inputs take the TMA path; others are loaded with ordinary loads.
+ *
+ * Workspace: pass NULL to use a workspace the library owns (one per device and
+ * stream, grown on demand -- growth calls cudaMalloc, so size it up front with a
+ * first call outside stream capture), or pass a device buffer of at least
+ * sleek_*_workspace_size() bytes.  The library clears the part it uses with
+ * cudaMemsetAsync on the same stream before each launch.  Calls that share one
+ * workspace must be ordered on one stream.
+ */
+#ifndef SLEEK_CAPI_H
+#define SLEEK_CAPI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SLEEK_OK                 0
+#define SLEEK_ERR_INVALID_ARG    1  /* null pointer, negative size, size not a multiple of the element */
+#define SLEEK_ERR_ALIGNMENT      2  /* pointer not aligned as documented above */
+#define SLEEK_ERR_CUDA           3  /* a CUDA runtime call failed (launch, memset, allocation) */
+#define SLEEK_ERR_ERROR_BOUND    4  /* error bound too large (the reference exits, sleek_lossy_gpu.h:68) */
+#define SLEEK_ERR_CORRUPT_STREAM 5  /* malformed stream (the reference traps, sleek_common_gpu.h:753,1264) */
+#define SLEEK_ERR_TIMEOUT        6  /* a device-side wait exceeded its time limit */
+#define SLEEK_ERR_WORKSPACE      7  /* caller workspace smaller than required */
+#define SLEEK_ERR_NO_DEVICE      8  /* no CUDA device */
+#define SLEEK_ERR_CAPACITY       9  /* output buffer smaller than required */
+
+/* Human-readable name of a status code. */
+const char* sleek_status_string(int status);
+
+/* Replaces sleek_upper_bound_size (include/sleek_common_gpu.h:79-83): bytes to
+ * allocate for a stream of an insize-byte input: 12 + 2*chunks + 16384*chunks. */
+long long sleek_upper_bound_size(long long insize);
+
+/* Replaces sleek_system_checks (include/sleek_common_gpu.h:86-105): 0 when the
+ * host is little-endian with the expected integer sizes, -1 otherwise. */
+int sleek_system_checks(void);
+
+/* Replaces sleek_thread_blocks (include/sleek_common_gpu.h:108-119): the
+ * persistent grid size this library uses on the current device (the reference
+ * value is accepted and ignored by the compress / decompress calls). */
+int sleek_thread_blocks(void);
+
+/* Workspace bytes for one compress of insize bytes / one decompress. */
+size_t sleek_compress_workspace_size(long long insize);
+size_t sleek_decompress_workspace_size(void);
+
+/* Error-bound parameters; replace sleek_error_bound_info<T> and
+ * sleek_error_bound<F> (include/sleek_lossy_gpu.h:47-71).  The sign of eb is
+ * ignored, as in the reference.  Returns SLEEK_ERR_ERROR_BOUND where the
+ * reference would exit(-1). */
+typedef struct { int eb_e; int thr_e; unsigned int offs_e; } sleek_eb_info_f32;
+typedef struct { int eb_e; int thr_e; unsigned long long offs_e; } sleek_eb_info_f64;
+int sleek_error_bound_f32(float eb, sleek_eb_info_f32* info);
+int sleek_error_bound_f64(double eb, sleek_eb_info_f64* info);
+
+/* Lossless compress; replaces sleek_compress_gpu(blocks, const float* or const double*, ...)
+ * (include/sleek_lossless_gpu.h:47-60, 75-88).  d_encoded must hold
+ * sleek_upper_bound_size(num_elements * elemsize) bytes; *d_encsize (device)
+ * receives the stream size in bytes. */
+int sleek_compress_f32(const float* d_input, long long num_elements, unsigned char* d_encoded,
+                       long long* d_encsize, void* d_workspace, size_t workspace_bytes, void* stream);
+int sleek_compress_f64(const double* d_input, long long num_elements, unsigned char* d_encoded,
+                       long long* d_encsize, void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Lossless decompress; replaces sleek_decompress_gpu(blocks, const byte*, float* or double*, ...)
+ * (include/sleek_lossless_gpu.h:63-72, 91-100).  encoded_bytes bounds every read
+ * of the stream and decoded_capacity bounds the output (pass -1 for either to
+ * trust the stream, as the reference does); *d_decsize (device) receives the
+ * decoded size in bytes. */
+int sleek_decompress_f32(const unsigned char* d_encoded, long long encoded_bytes, float* d_decoded,
+                         long long decoded_capacity, long long* d_decsize, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+int sleek_decompress_f64(const unsigned char* d_encoded, long long encoded_bytes, double* d_decoded,
+                         long long decoded_capacity, long long* d_decsize, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* Absolute-error-bounded lossy compress / decompress; replace the
+ * sleek_error_bound_info overloads (include/sleek_lossy_gpu.h:74-99, 102-127).
+ * Decompress needs the same eb parameters that compress used (the stream does
+ * not record them). */
+int sleek_compress_lossy_f32(sleek_eb_info_f32 eb, const float* d_input, long long num_elements,
+                             unsigned char* d_encoded, long long* d_encsize, void* d_workspace,
+                             size_t workspace_bytes, void* stream);
+int sleek_compress_lossy_f64(sleek_eb_info_f64 eb, const double* d_input, long long num_elements,
+                             unsigned char* d_encoded, long long* d_encsize, void* d_workspace,
+                             size_t workspace_bytes, void* stream);
+int sleek_decompress_lossy_f32(sleek_eb_info_f32 eb, const unsigned char* d_encoded, long long encoded_bytes,
+                               float* d_decoded, long long decoded_capacity, long long* d_decsize,
+                               void* d_workspace, size_t workspace_bytes, void* stream);
+int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* d_encoded, long long encoded_bytes,
+                               double* d_decoded, long long decoded_capacity, long long* d_decsize,
+                               void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Synchronises `stream` and reads the device status of the last call that used
+ * d_workspace (NULL = the library-owned workspace of the current device and
+ * `stream`).  *status receives SLEEK_OK or the first device-side error. */
+int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLEEK_CAPI_H */

@@ -1,0 +1,88 @@
+"""ctypes binding of the C ABI in ``include/sleek_capi.h``.
+
+Loads ``sleek_b200/_lib/libsleek_b200.so`` (built by ``sleek_b200/build.py``).
+There is no fallback: if the library is missing or cannot be loaded, importing
+the binding raises, so a box without the CUDA build fails loudly instead of
+silently computing something else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+SLEEK_OK = 0
+SLEEK_ERR_INVALID_ARG = 1
+SLEEK_ERR_ALIGNMENT = 2
+SLEEK_ERR_CUDA = 3
+SLEEK_ERR_ERROR_BOUND = 4
+SLEEK_ERR_CORRUPT_STREAM = 5
+SLEEK_ERR_TIMEOUT = 6
+SLEEK_ERR_WORKSPACE = 7
+SLEEK_ERR_NO_DEVICE = 8
+SLEEK_ERR_CAPACITY = 9
+
+
+class EbInfoF32(C.Structure):
+    _fields_ = [("eb_e", C.c_int), ("thr_e", C.c_int), ("offs_e", C.c_uint)]
+
+
+class EbInfoF64(C.Structure):
+    _fields_ = [("eb_e", C.c_int), ("thr_e", C.c_int), ("offs_e", C.c_ulonglong)]
+
+
+# every symbol the header declares: name -> (restype, argtypes)
+_i64 = C.c_longlong
+_vp = C.c_void_p
+_sz = C.c_size_t
+SIGNATURES = {
+    "sleek_status_string": (C.c_char_p, [C.c_int]),
+    "sleek_upper_bound_size": (_i64, [_i64]),
+    "sleek_system_checks": (C.c_int, []),
+    "sleek_thread_blocks": (C.c_int, []),
+    "sleek_compress_workspace_size": (_sz, [_i64]),
+    "sleek_decompress_workspace_size": (_sz, []),
+    "sleek_error_bound_f32": (C.c_int, [C.c_float, C.POINTER(EbInfoF32)]),
+    "sleek_error_bound_f64": (C.c_int, [C.c_double, C.POINTER(EbInfoF64)]),
+    "sleek_compress_f32": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "sleek_compress_f64": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "sleek_decompress_f32": (C.c_int, [_vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "sleek_decompress_f64": (C.c_int, [_vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "sleek_compress_lossy_f32": (C.c_int, [EbInfoF32, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "sleek_compress_lossy_f64": (C.c_int, [EbInfoF64, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "sleek_decompress_lossy_f32": (C.c_int, [EbInfoF32, _vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "sleek_decompress_lossy_f64": (C.c_int, [EbInfoF64, _vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
+    "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises OSError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with `python -m sleek_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (rt, at) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = rt
+            f.argtypes = at
+        _lib = L
+    return _lib
+
+
+class SleekError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        self.status = int(status)
+        msg = lib().sleek_status_string(self.status).decode()
+        super().__init__(f"{where}: {msg} (status {self.status})" if where else f"{msg} (status {self.status})")
+
+
+def check(status: int, where: str = "") -> None:
+    if status != SLEEK_OK:
+        raise SleekError(status, where)

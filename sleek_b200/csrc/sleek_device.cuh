@@ -1,0 +1,422 @@
+// sleek_device.cuh -- device building blocks of the sm_100a SLEEK codec.
+//
+// Everything here is integer / bit arithmetic.  The value transforms restate the
+// reference's arithmetic exactly (that is what makes the byte stream identical);
+// the data movement (TMA bulk loads into shared memory, gather-form bit packing,
+// bounded decoupled look-back, 16-byte shifted stores) is this project's own.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sleek_launch.h"
+
+namespace sleek {
+
+constexpr int CS = 16384;          // chunk bytes; fixed by the stream format
+constexpr int SC = 32;             // subchunks per chunk; fixed by the stream format
+constexpr int STAGE_BYTES = CS + 64;  // one chunk plus room for a 16-byte misaligned window
+
+// status codes shared with the C ABI (include/sleek_capi.h)
+constexpr unsigned ST_CORRUPT = 5;
+constexpr unsigned ST_TIMEOUT = 6;
+constexpr unsigned ST_CAPACITY = 9;
+
+// workspace header words (u64 each), followed by the look-back flag array
+enum WsWord { WS_TICKET = 0, WS_DONE = 1, WS_STATUS = 2, WS_TOTAL = 3, WS_ERRPOS = 4, WS_HDR_WORDS = 32 };
+
+// look-back flag: state in bits 62-63, value in bits 0-61
+constexpr uint64_t FLAG_AGG = 1ull << 62;
+constexpr uint64_t FLAG_INC = 2ull << 62;
+constexpr uint64_t FLAG_VAL = (1ull << 62) - 1;
+
+constexpr unsigned long long SPIN_TIMEOUT_NS = 4000000000ull;  // 4 s of wall time per wait
+
+// ----------------------------------------------------------------------------
+// value traits
+// ----------------------------------------------------------------------------
+template <typename T> struct VT;
+template <> struct VT<uint32_t> {
+  static constexpr int TB = 32;            // bits per value
+  static constexpr int VPC = CS / 4;       // values per chunk
+  static constexpr int VPS = VPC / SC;     // values per subchunk (128)
+  static constexpr int WPS_PER_LN = 2;     // packed u64 words per subchunk per bit of width
+};
+template <> struct VT<uint64_t> {
+  static constexpr int TB = 64;
+  static constexpr int VPC = CS / 8;
+  static constexpr int VPS = VPC / SC;     // 64
+  static constexpr int WPS_PER_LN = 1;
+};
+
+// ----------------------------------------------------------------------------
+// PTX helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init()
+{
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity; gives up after SPIN_TIMEOUT_NS.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > SPIN_TIMEOUT_NS) return false;
+  }
+  return true;
+}
+
+// 1-D bulk copy global -> shared (no multicast); completion counted on `bar`.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p)
+{
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v)
+{
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p)
+{
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// records the first error; later errors keep the first code
+__device__ __forceinline__ void set_status(uint64_t* ws, unsigned code, long long pos)
+{
+  if (atomicCAS(reinterpret_cast<unsigned long long*>(&ws[WS_STATUS]), 0ull, (unsigned long long)code) == 0ull) {
+    atomicExch(reinterpret_cast<unsigned long long*>(&ws[WS_ERRPOS]), (unsigned long long)pos);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// value transforms (restated from include/sleek_common_gpu.h of the reference:
+// lossless forward :356-374, inverse :614-632, quantize :776-802, deQuantize
+// :1077-1108).  Bit-exactness of the stream depends on these being identical.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t fwd(uint32_t v)
+{
+  v = (v << 1) | (v >> 31);
+  if (v & 0xff000000u) {
+    v -= 0x80000000u;
+    if (((v & 0xff000000u) == 0u) | (v >= 0x80000000u)) v -= 0x01000000u;
+  }
+  return (v << 1) ^ static_cast<uint32_t>(static_cast<int32_t>(v) >> 31);
+}
+
+__device__ __forceinline__ uint64_t fwd(uint64_t v)
+{
+  v = (v << 1) | (v >> 63);
+  if (v & 0xffe0000000000000ull) {
+    v -= 0x8000000000000000ull;
+    if (((v & 0xffe0000000000000ull) == 0ull) | (v >= 0x8000000000000000ull)) v -= 0x0020000000000000ull;
+  }
+  return (v << 1) ^ static_cast<uint64_t>(static_cast<int64_t>(v) >> 63);
+}
+
+__device__ __forceinline__ uint32_t inv(uint32_t v)
+{
+  v = (v >> 1) ^ static_cast<uint32_t>(static_cast<int32_t>(v << 31) >> 31);
+  if (v & 0xff000000u) {
+    if (v >= 0x80000000u) v += 0x01000000u;
+    v += 0x80000000u;
+  }
+  return (v << 31) | (v >> 1);
+}
+
+__device__ __forceinline__ uint64_t inv(uint64_t v)
+{
+  v = (v >> 1) ^ static_cast<uint64_t>(static_cast<int64_t>(v << 63) >> 63);
+  if (v & 0xffe0000000000000ull) {
+    if (v >= 0x8000000000000000ull) v += 0x0020000000000000ull;
+    v += 0x8000000000000000ull;
+  }
+  return (v << 63) | (v >> 1);
+}
+
+__device__ __forceinline__ uint32_t quant(uint32_t val, const QParams& q)
+{
+  const uint32_t a = val & 0x7fffffffu;
+  const int ve = static_cast<int>(a >> 23);
+  uint32_t enc = 0;
+  if (ve >= q.thr_e) {
+    enc = a - static_cast<uint32_t>(q.offs);
+  } else if (ve >= q.eb_e) {
+    const int sh = q.thr_e - ve;
+    const uint32_t mant = ((val & 0x007fffffu) | 0x00800000u) + (1u << (sh - 1));
+    enc = mant >> sh;
+  }
+  enc = (enc << 1) | ((~val) >> 31);
+  return enc ? enc - 1u : 0u;
+}
+
+__device__ __forceinline__ uint64_t quant(uint64_t val, const QParams& q)
+{
+  const uint64_t a = val & 0x7fffffffffffffffull;
+  const int ve = static_cast<int>(a >> 52);
+  uint64_t enc = 0;
+  if (ve >= q.thr_e) {
+    enc = a - q.offs;
+  } else if (ve >= q.eb_e) {
+    const int sh = q.thr_e - ve;
+    const uint64_t mant = ((val & 0x000fffffffffffffull) | 0x0010000000000000ull) + (1ull << (sh - 1));
+    enc = mant >> sh;
+  }
+  enc = (enc << 1) | ((~val) >> 63);
+  return enc ? enc - 1ull : 0ull;
+}
+
+__device__ __forceinline__ uint32_t dequant(uint32_t enc, const QParams& q)
+{
+  if (enc == 0u) return 0u;
+  const uint32_t a = (enc + 1u) >> 1;
+  uint32_t dec = 0;
+  if (a >= (1u << 23)) {
+    dec = a + static_cast<uint32_t>(q.offs);
+  } else if (a > 0u) {
+    const int sh = __clz(a) - 8;
+    dec = ((a << sh) & 0x007fffffu) | (static_cast<uint32_t>(q.thr_e - sh) << 23);
+  }
+  return dec | (enc << 31);
+}
+
+__device__ __forceinline__ uint64_t dequant(uint64_t enc, const QParams& q)
+{
+  if (enc == 0ull) return 0ull;
+  const uint64_t a = (enc + 1ull) >> 1;
+  uint64_t dec = 0;
+  if (a >= (1ull << 52)) {
+    dec = a + q.offs;
+  } else if (a > 0ull) {
+    const int sh = __clzll(a) - 11;
+    dec = ((a << sh) & 0x000fffffffffffffull) | (static_cast<uint64_t>(q.thr_e - sh) << 52);
+  }
+  return dec | (enc << 63);
+}
+
+template <bool LOSSY, typename T>
+__device__ __forceinline__ T encode_value(T v, const QParams& q)
+{
+  if constexpr (LOSSY) return quant(v, q);
+  else return fwd(v);
+}
+
+template <bool LOSSY, typename T>
+__device__ __forceinline__ T decode_value(T v, const QParams& q)
+{
+  if constexpr (LOSSY) return dequant(v, q);
+  else return inv(v);
+}
+
+__device__ __forceinline__ int bit_width(uint32_t m) { return m ? 32 - __clz(m) : 0; }
+__device__ __forceinline__ int bit_width(uint64_t m) { return m ? 64 - __clzll(m) : 0; }
+
+__device__ __forceinline__ uint32_t warp_max(uint32_t v) { return __reduce_max_sync(0xffffffffu, v); }
+__device__ __forceinline__ uint64_t warp_max(uint64_t v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint64_t w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ long long warp_sum(long long v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// padded index of value k in the transformed-value buffer (one pad slot per 32
+// values keeps the gather reads of the packer on distinct banks)
+__device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
+
+// ----------------------------------------------------------------------------
+// Decoupled look-back over flag words.  Called by one whole warp for item
+// `idx` whose segment starts at `seg_begin` (items before the segment count as
+// an inclusive prefix of 0).  Returns the exclusive prefix, or -1 when a wait
+// exceeded SPIN_TIMEOUT_NS or another CTA already reported an error.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ long long lookback(const uint64_t* flags, long long idx, long long seg_begin,
+                                              const uint64_t* ws)
+{
+  const int lane = threadIdx.x & 31;
+  long long excl = 0;
+  long long end = idx - 1;
+  unsigned long long t0 = 0;
+  unsigned sleep_ns = 32;
+  int polls = 0;
+  while (true) {
+    const long long j = end - lane;
+    const uint64_t f = (j >= seg_begin) ? ld_acquire_u64(&flags[j]) : FLAG_INC;
+    const unsigned st = static_cast<unsigned>(f >> 62);
+    const unsigned notready = __ballot_sync(0xffffffffu, st == 0u);
+    const unsigned incl = __ballot_sync(0xffffffffu, st == 2u);
+    const unsigned usable = notready ? ((notready & (0u - notready)) - 1u) : 0xffffffffu;
+    const unsigned inc_usable = incl & usable;
+    if (inc_usable) {
+      const int p = __ffs(inc_usable) - 1;
+      excl += warp_sum(lane <= p ? static_cast<long long>(f & FLAG_VAL) : 0ll);
+      return excl;
+    }
+    if (usable) {  // a run of aggregates nearest to us: consume it and slide
+      const int z = notready ? __ffs(notready) - 1 : 32;
+      excl += warp_sum(lane < z ? static_cast<long long>(f & FLAG_VAL) : 0ll);
+      end -= z;
+      continue;
+    }
+    // nearest predecessor not ready yet: back off, bounded in time
+    if (++polls == 64) {
+      t0 = globaltimer_ns();
+    } else if (polls > 64 && (polls & 63) == 0) {
+      const bool late = globaltimer_ns() - t0 > SPIN_TIMEOUT_NS;
+      const bool failed = ld_relaxed_u64(&ws[WS_STATUS]) != 0ull;
+      if (__any_sync(0xffffffffu, late || failed)) return -1;
+    }
+    if (polls > 8) {
+      __nanosleep(sleep_ns);
+      if (sleep_ns < 1024) sleep_ns <<= 1;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Shifted store: writes `len` bytes from 16-byte aligned shared memory `src`
+// to the arbitrary global byte address `dst`.  Whole aligned 16-byte granules
+// use one vector store; the (at most two) granules shared with neighbouring
+// chunks are written byte by byte.  Called by all NT threads.
+// ----------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len)
+{
+  const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
+  const int sft = static_cast<int>(d & 15u);
+  uint8_t* const a0 = dst - sft;
+  const int nunits = (sft + len + 15) >> 4;
+  const uint4* const s4 = reinterpret_cast<const uint4*>(src);
+  const int bo = (16 - sft) & 15;
+  const int wq = bo >> 2;
+  const int bb8 = (bo & 3) * 8;
+  for (int j = threadIdx.x; j < nunits; j += NT) {
+    const int r = 16 * j - sft;
+    if (r >= 0 && r + 16 <= len) {
+      uint4 o;
+      if (sft == 0) {
+        o = s4[j];
+      } else {
+        const uint4 x = s4[j - 1];
+        const uint4 y = s4[j];
+        uint32_t a[5];
+        switch (wq) {
+          case 0: a[0] = x.x; a[1] = x.y; a[2] = x.z; a[3] = x.w; a[4] = y.x; break;
+          case 1: a[0] = x.y; a[1] = x.z; a[2] = x.w; a[3] = y.x; a[4] = y.y; break;
+          case 2: a[0] = x.z; a[1] = x.w; a[2] = y.x; a[3] = y.y; a[4] = y.z; break;
+          default: a[0] = x.w; a[1] = y.x; a[2] = y.y; a[3] = y.z; a[4] = y.w; break;
+        }
+        o.x = __funnelshift_r(a[0], a[1], bb8);
+        o.y = __funnelshift_r(a[1], a[2], bb8);
+        o.z = __funnelshift_r(a[2], a[3], bb8);
+        o.w = __funnelshift_r(a[3], a[4], bb8);
+      }
+      *reinterpret_cast<uint4*>(a0 + 16 * j) = o;
+    } else {
+      const int b0 = r < 0 ? -r : 0;
+      const int b1 = (len - r) < 16 ? (len - r) : 16;
+      for (int b = b0; b < b1; b++) a0[16 * j + b] = src[r + b];
+    }
+  }
+}
+
+// Reads the u32 word starting at an arbitrary byte offset of 16-byte aligned
+// shared memory (the two aligned words around it, funnel-shifted).
+__device__ __forceinline__ uint32_t lds_u32_at_byte(const uint8_t* base, int byte_off)
+{
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(base);
+  const int wi = byte_off >> 2;
+  const int sh = (byte_off & 3) * 8;
+  return __funnelshift_r(w[wi], w[wi + 1], sh);
+}
+
+// Extracts `ln` bits (1 <= ln <= 64) starting at bit `pos` of 16-byte aligned
+// shared memory, LSB-first little-endian (the stream's bit order).
+__device__ __forceinline__ uint32_t extract_bits32(const uint32_t* w, int pos, int ln)
+{
+  const int wi = pos >> 5;
+  const uint32_t v = __funnelshift_r(w[wi], w[wi + 1], pos & 31);
+  return ln >= 32 ? v : (v & ((1u << ln) - 1u));
+}
+
+__device__ __forceinline__ uint64_t extract_bits64(const uint32_t* w, int pos, int ln)
+{
+  const int wi = pos >> 5;
+  const int sh = pos & 31;
+  const uint32_t w0 = w[wi], w1 = w[wi + 1], w2 = w[wi + 2];
+  const uint32_t lo = __funnelshift_r(w0, w1, sh);
+  const uint32_t hi = __funnelshift_r(w1, w2, sh);
+  const uint64_t v = (static_cast<uint64_t>(hi) << 32) | lo;
+  return ln >= 64 ? v : (v & ((1ull << ln) - 1ull));
+}
+
+}  // namespace sleek

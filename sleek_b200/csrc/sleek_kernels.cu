@@ -1,0 +1,587 @@
+// sleek_kernels.cu -- sm_100a encode / decode kernels for one buffer.
+//
+// Encode (replaces d_encode, include/sleek_common_gpu.h:474-559, 989-1074 of the
+// reference): persistent CTAs take 16 KB chunks by atomic ticket, in order.  A
+// chunk arrives in shared memory by a 1-D TMA bulk copy issued one chunk ahead;
+// warps transform a subchunk each (value arithmetic restated from the reference)
+// and take the bit width from a warp max; warp 0 scans the widths, publishes the
+// chunk's compressed size and runs a bounded decoupled look-back while the other
+// warps pack the chunk in gather form (each thread assembles whole 64-bit words,
+// no shared atomics); finally all threads store the chunk at its byte offset with
+// 16-byte vector stores.  A chunk whose encoding is not smaller than its input is
+// stored raw straight from the staged copy (never re-read from HBM).
+//
+// Decode (replaces d_decode, :688-768, 1199-1279): CTAs take contiguous chunk
+// ranges in ticket order, sum their ranges' compressed sizes, look back over the
+// preceding ranges once, then stream their chunks through a two-stage TMA
+// pipeline (each copy is the 16-byte aligned superset of the chunk's bytes) and
+// unpack with funnel shifts straight into coalesced global stores.  Malformed
+// streams set an error status instead of trapping.
+#include "sleek_device.cuh"
+#include "sleek_launch.h"
+
+namespace sleek {
+
+constexpr int TBUF_BYTES = 16896;  // (4096 + 128) u32 or (2048 + 64) u64, padded layout
+
+struct EncMisc {
+  uint64_t bar[2];
+  long long ticket[2];
+  long long excl;
+  int lnv[SC];
+  int cumw[SC + 1];
+  unsigned rcp[SC];
+  int csize;
+  int comp;
+  int abort;
+};
+
+constexpr int ENC_SMEM = 2 * STAGE_BYTES + TBUF_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
+
+template <typename T, bool LOSSY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_encode(const EncArgs a)
+{
+  using V = VT<T>;
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t* const stage0 = smem;
+  T* const tb = reinterpret_cast<T*>(smem + 2 * STAGE_BYTES);
+  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + 2 * STAGE_BYTES + TBUF_BYTES);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const long long chunks = (a.insize + CS - 1) / CS;
+  uint64_t* const ws = a.ws;
+  uint64_t* const flags = ws + WS_HDR_WORDS;
+  uint8_t* const size_out = a.out + 8;
+  uint8_t* const data_out = a.out + 8 + 2 * chunks;
+  const bool in_aligned = (reinterpret_cast<uintptr_t>(a.in) & 15u) == 0u;
+
+  auto issue = [&](long long c, int stg) {  // thread 0 only
+    const long long base = c * CS;
+    const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+    const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
+    if (tbytes) {
+      mbar_arrive_expect_tx(&m.bar[stg], tbytes);
+      tma_load_1d(stage0 + stg * STAGE_BYTES, a.in + base, tbytes, &m.bar[stg]);
+    } else {
+      mbar_arrive(&m.bar[stg]);
+    }
+  };
+
+  long long next_ticket = 0;
+  if (tid == 0) {
+    mbar_init(&m.bar[0], 1);
+    mbar_init(&m.bar[1], 1);
+    mbar_fence_init();
+    const long long t0 = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
+    next_ticket = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
+    m.ticket[0] = t0;
+    m.abort = 0;
+    if (t0 < chunks) issue(t0, 0);
+  }
+  __syncthreads();
+
+  for (int it = 0;; ++it) {
+    const int s = it & 1;
+    const long long c = m.ticket[s];
+    if (c >= chunks) break;
+    uint8_t* const stg = stage0 + s * STAGE_BYTES;
+
+    if (tid == 0) {  // prefetch the next ticket's chunk into the other stage
+      const long long t = next_ticket;
+      m.ticket[s ^ 1] = t;
+      if (t < chunks) {
+        issue(t, s ^ 1);
+        next_ticket = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
+      }
+    }
+
+    const bool arrived = mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
+    if (__syncthreads_or(!arrived)) {
+      if (tid == 0) set_status(ws, ST_TIMEOUT, c);
+      // let any copy still in flight into this CTA's shared memory land first
+      mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
+      mbar_wait_bounded(&m.bar[s ^ 1], ((it + 1) >> 1) & 1);
+      break;
+    }
+
+    // ---- phase A: transform / quantize, subchunk bit widths ----------------
+    const long long base = c * CS;
+    const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+    const int tbytes = in_aligned ? (osize & ~15) : 0;
+    {
+      T* const sv = reinterpret_cast<T*>(stg);
+      const T* const gin = reinterpret_cast<const T*>(a.in + base);
+      constexpr int PER = V::VPS / 32;
+      for (int i = warp; i < SC; i += NT / 32) {
+        T mx = 0;
+        if (tbytes == CS) {
+#pragma unroll
+          for (int u = 0; u < PER; ++u) {
+            const int k = i * V::VPS + u * 32 + lane;
+            const T e = encode_value<LOSSY>(sv[k], a.q);
+            tb[tpad(k)] = e;
+            mx = e > mx ? e : mx;
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < PER; ++u) {
+            const int k = i * V::VPS + u * 32 + lane;
+            const int b = k * static_cast<int>(sizeof(T));
+            T v = 0;
+            if (b < tbytes) {
+              v = sv[k];
+            } else if (b < osize) {
+              v = gin[k];
+              sv[k] = v;  // keep the staged copy complete for a raw store
+            }
+            const T e = encode_value<LOSSY>(v, a.q);  // zero padding is transformed too
+            tb[tpad(k)] = e;
+            mx = e > mx ? e : mx;
+          }
+        }
+        mx = warp_max(mx);
+        if (lane == 0) m.lnv[i] = bit_width(mx);
+      }
+    }
+    __syncthreads();
+
+    // ---- widths scan, size decision, publish aggregate ----------------------
+    if (warp == 0) {
+      const int ln = m.lnv[lane];
+      const int wc = ln * V::WPS_PER_LN;
+      int incl = wc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      m.cumw[lane + 1] = incl;
+      m.rcp[lane] = ln > 1 ? static_cast<unsigned>(((1ull << 32) + ln - 1) / ln) : 0u;
+      if (lane == 0) m.cumw[0] = 0;
+      const int W = __shfl_sync(0xffffffffu, incl, 31);
+      const int newsize = 34 + 8 * W;
+      const bool comp = newsize < osize;
+      const int csize = comp ? newsize : osize;
+      if (lane == 0) {
+        m.csize = csize;
+        m.comp = comp;
+        st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+      }
+    }
+    __syncthreads();
+
+    const int csize = m.csize;
+    const bool comp = m.comp != 0;
+    const int W = m.cumw[SC];
+
+    // ---- look-back (warp 0)  ||  gather-form packing (warps 1..) ------------
+    if (warp == 0) {
+      long long excl = 0;
+      if (c > 0) {
+        excl = lookback(flags, c, 0, ws);
+        unsigned err = 0;
+        if (excl < 0) err = ST_TIMEOUT;
+        else if (excl > c * CS) err = ST_CAPACITY;
+        if (err) {
+          if (lane == 0) set_status(ws, err, c);
+          excl = -1;
+        }
+        // an impossible prefix is replaced by the largest legal one so that
+        // every later chunk still writes inside the output bound
+        if (lane == 0)
+          st_release_u64(&flags[c], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
+      }
+      if (lane == 0) {
+        m.excl = excl;
+        if (c == chunks - 1 && excl >= 0) ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
+      }
+      if (comp) {
+        stg[lane] = static_cast<uint8_t>(m.lnv[lane]);
+        if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 8 * W) = static_cast<int16_t>(osize);
+      }
+    } else if (comp) {
+      uint64_t* const pw = reinterpret_cast<uint64_t*>(stg + 32);
+      for (int g = tid - 32; g < W; g += NT - 32) {
+        int i = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (m.cumw[i + step] <= g) i += step;
+        const int ln = m.lnv[i];
+        const int start = (g - m.cumw[i]) * 64;
+        int k = ln > 1 ? static_cast<int>(__umulhi(static_cast<unsigned>(start), m.rcp[i])) : start;
+        const int off = k * ln - start;  // in (-ln, 0]
+        const int kb = i * V::VPS;
+        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
+        int n = ln + off;
+        ++k;
+        while (n < 64 && k < V::VPS) {
+          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
+          n += ln;
+          ++k;
+        }
+        pw[g] = acc;
+      }
+    }
+    __syncthreads();
+
+    // ---- store the chunk at its byte offset ----------------------------------
+    const long long excl = m.excl;
+    if (excl >= 0) {
+      store_shifted<NT>(data_out + excl, stg, csize);
+      if (tid == 0) *reinterpret_cast<uint16_t*>(size_out + 2 * c) = static_cast<uint16_t>(csize);
+    }
+    fence_proxy_async_smem();  // generic accesses of this stage before the next TMA write
+    __syncthreads();
+  }
+
+  // ---- epilogue: the last CTA out writes the header and the stream size ------
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
+    if (d == gridDim.x - 1) {
+      __threadfence();
+      const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+      const long long total = chunks ? static_cast<long long>(ld_relaxed_u64(&ws[WS_TOTAL])) : 0ll;
+      *reinterpret_cast<long long*>(a.out) = a.insize;
+      *a.outsize = st ? -static_cast<long long>(st) : 8 + 2 * chunks + total;
+    }
+  }
+}
+
+// ============================================================================
+// decode
+// ============================================================================
+struct DecChunk {
+  long long c;
+  long long off;
+  int cs;
+  int sft;
+  int ok;
+  int pad_;
+};
+
+struct DecMisc {
+  uint64_t bar[2];
+  DecChunk info[2];
+  long long excl;
+  long long vb;
+  long long red[NT_MAX_WARPS];
+  int bad[NT_MAX_WARPS];
+  int lnv[SC];
+  int bitbase[SC];
+  int ok;
+  int abort;
+};
+
+constexpr int DEC_SMEM = 2 * STAGE_BYTES + ((sizeof(DecMisc) + 127) / 128) * 128;
+
+__device__ __forceinline__ uint64_t lds_u64_at_byte(const uint8_t* base, int byte_off)
+{
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(base);
+  const int wi = byte_off >> 2;
+  const int sh = (byte_off & 3) * 8;
+  const uint32_t lo = __funnelshift_r(w[wi], w[wi + 1], sh);
+  const uint32_t hi = __funnelshift_r(w[wi + 1], w[wi + 2], sh);
+  return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+template <typename T, bool LOSSY, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
+{
+  using V = VT<T>;
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t* const stage0 = smem;
+  DecMisc& m = *reinterpret_cast<DecMisc*>(smem + 2 * STAGE_BYTES);
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  uint64_t* const ws = a.ws;
+  uint64_t* const flags = ws + WS_HDR_WORDS;
+
+  // header checks (every CTA reads the 8-byte header)
+  const long long insize = *reinterpret_cast<const long long*>(a.in);
+  const long long chunks = insize > 0 ? (insize + CS - 1) / CS : 0;
+  bool hdr_ok = insize >= 0 && (insize % static_cast<long long>(sizeof(T))) == 0;
+  if (a.in_len >= 0 && 8 + 2 * chunks > a.in_len) hdr_ok = false;
+  const bool cap_ok = a.out_cap < 0 || insize <= a.out_cap;
+  const long long payload_len = a.in_len >= 0 ? a.in_len - 8 - 2 * chunks : -1;
+  const uint16_t* const size_in = reinterpret_cast<const uint16_t*>(a.in + 8);
+  const uint8_t* const data_in = a.in + 8 + 2 * chunks;
+
+  if (tid == 0) {
+    mbar_init(&m.bar[0], 1);
+    mbar_init(&m.bar[1], 1);
+    mbar_fence_init();
+    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
+    m.abort = 0;
+    if (!hdr_ok) set_status(ws, ST_CORRUPT, -1);
+    else if (!cap_ok) set_status(ws, ST_CAPACITY, -1);
+  }
+  __syncthreads();
+
+  const bool go = hdr_ok && cap_ok;
+  const long long vb = m.vb;
+  const long long K = (chunks + gridDim.x - 1) / gridDim.x;
+  const long long c0 = go ? min(vb * K, chunks) : 0;
+  const long long c1 = go ? min(c0 + K, chunks) : 0;
+
+  // ---- range aggregate + size-table validation ---------------------------------
+  {
+    long long sum = 0;
+    int bad = 0;
+    for (long long c = c0 + tid; c < c1; c += NT) {
+      const int cs = size_in[c];
+      const int os = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+      bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
+      sum += cs;
+    }
+    sum = warp_sum(sum);
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      m.red[warp] = sum;
+      m.bad[warp] = bad;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      long long s2 = lane < NW ? m.red[lane] : 0;
+      int b2 = lane < NW ? m.bad[lane] : 0;
+      s2 = warp_sum(s2);
+      b2 = __any_sync(0xffffffffu, b2);
+      if (b2 && lane == 0) set_status(ws, ST_CORRUPT, c0);
+      if (lane == 0) st_release_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
+      long long excl = 0;
+      if (vb > 0) {
+        excl = lookback(flags, vb, 0, ws);
+        if (excl < 0) {
+          if (lane == 0) set_status(ws, ST_TIMEOUT, c0);
+        }
+        if (lane == 0)
+          st_release_u64(&flags[vb], FLAG_INC | (static_cast<uint64_t>(excl >= 0 ? excl + s2 : 0) & FLAG_VAL));
+      }
+      if (lane == 0) m.excl = b2 ? -1 : excl;
+    }
+    __syncthreads();
+  }
+
+  const long long excl = m.excl;
+  if (excl >= 0 && c0 < c1) {
+    // producer state (warp 0): offsets and sizes of a window of 32 chunks
+    long long wbase = -64, woff = 0, run = excl;
+    int wcs = 0;
+    auto issue = [&](long long c, int stg) {  // warp 0, warp-uniform
+      if (c - wbase >= 32) {
+        wbase = c;
+        const long long cc = c + lane;
+        const int cs = cc < c1 ? static_cast<int>(size_in[cc]) : 0;
+        long long incl = cs;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        woff = run + incl - cs;
+        wcs = cs;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      const int l = static_cast<int>(c - wbase);
+      const long long off = __shfl_sync(0xffffffffu, woff, l);
+      const int cs = __shfl_sync(0xffffffffu, wcs, l);
+      if (lane == 0) {
+        const uint8_t* src = data_in + off;
+        const int sft = static_cast<int>(reinterpret_cast<uintptr_t>(src) & 15u);
+        const uint32_t nb = static_cast<uint32_t>((sft + cs + 15) & ~15);
+        const bool ok = cs >= 1 && cs <= CS && (payload_len < 0 || off + cs <= payload_len);
+        DecChunk& d = m.info[stg];
+        d.c = c;
+        d.off = off;
+        d.cs = cs;
+        d.sft = sft;
+        d.ok = ok;
+        if (ok) {
+          mbar_arrive_expect_tx(&m.bar[stg], nb);
+          tma_load_1d(stage0 + stg * STAGE_BYTES, src - sft, nb, &m.bar[stg]);
+        } else {
+          mbar_arrive(&m.bar[stg]);
+        }
+      }
+    };
+
+    if (warp == 0) issue(c0, 0);
+    int it = 0;
+    for (long long c = c0; c < c1; ++c, ++it) {
+      const int s = it & 1;
+      uint8_t* const stg = stage0 + s * STAGE_BYTES;
+      if (warp == 0 && c + 1 < c1) issue(c + 1, s ^ 1);
+
+      const bool arrived = mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
+      if (__syncthreads_or(!arrived)) {
+        if (tid == 0) set_status(ws, ST_TIMEOUT, c);
+        mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
+        if (c + 1 < c1) mbar_wait_bounded(&m.bar[s ^ 1], ((it + 1) >> 1) & 1);
+        break;
+      }
+
+      const DecChunk d = m.info[s];
+      const int osize = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+      uint8_t* const outc = a.out + c * CS;
+      if (!d.ok) {
+        if (tid == 0) set_status(ws, ST_CORRUPT, c);
+      } else if (d.cs == osize) {
+        // raw chunk: shifted copy from the staged bytes
+        T* const o = reinterpret_cast<T*>(outc);
+        const int nv = osize / static_cast<int>(sizeof(T));
+        for (int e = tid; e < nv; e += NT) {
+          if constexpr (sizeof(T) == 4) o[e] = lds_u32_at_byte(stg, d.sft + 4 * e);
+          else o[e] = lds_u64_at_byte(stg, d.sft + 8 * e);
+        }
+      } else {
+        if (warp == 0) {
+          const int ln = stg[d.sft + lane];
+          const int bitsw = ln * V::VPS;
+          int incl = bitsw;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+          }
+          const int tot = __shfl_sync(0xffffffffu, incl, 31);
+          m.lnv[lane] = ln;
+          m.bitbase[lane] = 8 * d.sft + 256 + incl - bitsw;
+          const bool bad_ln = __any_sync(0xffffffffu, ln > V::TB);
+          if (lane == 0) {
+            bool ok = !bad_ln && (34 + tot / 8 == d.cs);
+            if (ok) {
+              const int16_t tr = static_cast<int16_t>(stg[d.sft + d.cs - 2] | (stg[d.sft + d.cs - 1] << 8));
+              ok = tr == osize;
+            }
+            m.ok = ok;
+            if (!ok) set_status(ws, ST_CORRUPT, c);
+          }
+        }
+        __syncthreads();
+        if (m.ok) {
+          const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
+          T* const o = reinterpret_cast<T*>(outc);
+          const int nv = osize / static_cast<int>(sizeof(T));
+          for (int k = tid; k < nv; k += NT) {
+            const int i = k / V::VPS;
+            const int j = k - i * V::VPS;
+            const int ln = m.lnv[i];
+            T e = 0;
+            if (ln) {
+              if constexpr (sizeof(T) == 4) e = extract_bits32(w, m.bitbase[i] + j * ln, ln);
+              else e = extract_bits64(w, m.bitbase[i] + j * ln, ln);
+            }
+            o[k] = decode_value<LOSSY>(e, a.q);
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+    }
+  }
+
+  // ---- epilogue ------------------------------------------------------------------
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
+    if (dn == gridDim.x - 1) {
+      __threadfence();
+      const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+      *a.outsize = st ? -static_cast<long long>(st) : insize;
+    }
+  }
+}
+
+// ============================================================================
+// launchers
+// ============================================================================
+// Sets the dynamic shared memory limit of `k` once per device.
+template <typename K>
+static cudaError_t ensure_smem_attr(K k, int bytes, unsigned long long* done_mask)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (__atomic_load_n(done_mask, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) __atomic_fetch_or(done_mask, bit, __ATOMIC_RELEASE);
+  return e;
+}
+
+template <typename T, bool LOSSY>
+static cudaError_t launch_encode_t(const EncArgs& a, int grid, cudaStream_t st)
+{
+  constexpr int NT = 256, MINB = 4;
+  auto k = k_encode<T, LOSSY, NT, MINB>;
+  static unsigned long long attr = 0;
+  cudaError_t e = ensure_smem_attr(k, ENC_SMEM, &attr);
+  if (e != cudaSuccess) return e;
+  k<<<grid, NT, ENC_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, bool LOSSY>
+static cudaError_t launch_decode_t(const DecArgs& a, int grid, cudaStream_t st)
+{
+  constexpr int NT = 256, MINB = 4;
+  auto k = k_decode<T, LOSSY, NT, MINB>;
+  static unsigned long long attr = 0;
+  cudaError_t e = ensure_smem_attr(k, DEC_SMEM, &attr);
+  if (e != cudaSuccess) return e;
+  k<<<grid, NT, DEC_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T, bool LOSSY>
+static int occupancy_t(bool enc)
+{
+  int n = 0;
+  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<T, LOSSY, 256, 4>, 256, ENC_SMEM);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decode<T, LOSSY, 256, 4>, 256, DEC_SMEM);
+  return n;
+}
+
+cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cudaStream_t st)
+{
+  if (width == 4) return lossy ? launch_encode_t<uint32_t, true>(a, grid, st) : launch_encode_t<uint32_t, false>(a, grid, st);
+  return lossy ? launch_encode_t<uint64_t, true>(a, grid, st) : launch_encode_t<uint64_t, false>(a, grid, st);
+}
+
+cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st)
+{
+  if (width == 4) return lossy ? launch_decode_t<uint32_t, true>(a, grid, st) : launch_decode_t<uint32_t, false>(a, grid, st);
+  return lossy ? launch_decode_t<uint64_t, true>(a, grid, st) : launch_decode_t<uint64_t, false>(a, grid, st);
+}
+
+int blocks_per_sm(int width, bool lossy, bool enc)
+{
+  // the smem attribute must be set before the occupancy query counts dynamic smem
+  if (width == 4) {
+    if (lossy) {
+      cudaFuncSetAttribute(k_encode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+      cudaFuncSetAttribute(k_decode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
+      return occupancy_t<uint32_t, true>(enc);
+    }
+    cudaFuncSetAttribute(k_encode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_decode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
+    return occupancy_t<uint32_t, false>(enc);
+  }
+  if (lossy) {
+    cudaFuncSetAttribute(k_encode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_decode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
+    return occupancy_t<uint64_t, true>(enc);
+  }
+  cudaFuncSetAttribute(k_encode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+  cudaFuncSetAttribute(k_decode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
+  return occupancy_t<uint64_t, false>(enc);
+}
+
+}  // namespace sleek

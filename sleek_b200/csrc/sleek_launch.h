@@ -1,0 +1,43 @@
+// sleek_launch.h -- host-side launch interface between the C ABI (sleek_capi.cu)
+// and the kernels (sleek_kernels.cu).  Internal to the library.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sleek {
+
+constexpr int NT_MAX_WARPS = 32;
+
+// lossy quantizer parameters, as sleek_error_bound derives them
+// (include/sleek_lossy_gpu.h:47-71 of the reference)
+struct QParams {
+  int eb_e;
+  int thr_e;
+  uint64_t offs;
+};
+
+struct EncArgs {
+  const uint8_t* in;     // device input values (element aligned)
+  long long insize;      // input bytes
+  uint8_t* out;          // device stream, >= upper bound size, 8-byte aligned
+  long long* outsize;    // device: stream bytes, or -status on a device-detected error
+  uint64_t* ws;          // zeroed workspace: header words + one flag per chunk
+  QParams q;
+};
+
+struct DecArgs {
+  const uint8_t* in;     // device stream, 8-byte aligned
+  long long in_len;      // stream bytes, or -1 when unknown (no payload bound check)
+  uint8_t* out;          // device output values (element aligned)
+  long long out_cap;     // output capacity in bytes, or -1 when unknown
+  long long* outsize;    // device: decoded bytes, or -status
+  uint64_t* ws;          // zeroed workspace: header words + one flag per CTA
+  QParams q;
+};
+
+cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st);
+int blocks_per_sm(int width, bool lossy, bool enc);
+
+}  // namespace sleek
