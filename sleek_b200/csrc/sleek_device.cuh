@@ -296,12 +296,17 @@ __device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
 // ----------------------------------------------------------------------------
 // Decoupled look-back over flag words.  Called by one whole warp for item
 // `idx` whose segment starts at `seg_begin` (items before the segment count as
-// an inclusive prefix of 0).  Returns the exclusive prefix, or -1 when a wait
-// exceeded SPIN_TIMEOUT_NS or another CTA already reported an error.
+// an inclusive prefix of 0).  Each poll reads the 128 nearest unresolved flags
+// (four independent loads per lane), sums the run of aggregates up to the
+// nearest inclusive prefix, and slides past runs of aggregates; it only waits
+// when the nearest unresolved flag is not published yet.  Returns the exclusive
+// prefix, or -1 when a wait exceeded SPIN_TIMEOUT_NS or another CTA already
+// reported an error.
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ long long lookback(const uint64_t* flags, long long idx, long long seg_begin,
                                               const uint64_t* ws)
 {
+  constexpr int PER = 4;
   const int lane = threadIdx.x & 31;
   long long excl = 0;
   long long end = idx - 1;
@@ -309,25 +314,38 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
   unsigned sleep_ns = 32;
   int polls = 0;
   while (true) {
-    const long long j = end - lane;
-    const uint64_t f = (j >= seg_begin) ? ld_acquire_u64(&flags[j]) : FLAG_INC;
-    const unsigned st = static_cast<unsigned>(f >> 62);
-    const unsigned notready = __ballot_sync(0xffffffffu, st == 0u);
-    const unsigned incl = __ballot_sync(0xffffffffu, st == 2u);
-    const unsigned usable = notready ? ((notready & (0u - notready)) - 1u) : 0xffffffffu;
-    const unsigned inc_usable = incl & usable;
-    if (inc_usable) {
-      const int p = __ffs(inc_usable) - 1;
-      excl += warp_sum(lane <= p ? static_cast<long long>(f & FLAG_VAL) : 0ll);
-      return excl;
+    uint64_t f[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const long long j = end - lane - 32 * k;
+      f[k] = (j >= seg_begin) ? ld_relaxed_u64(&flags[j]) : FLAG_INC;
     }
-    if (usable) {  // a run of aggregates nearest to us: consume it and slide
-      const int z = notready ? __ffs(notready) - 1 : 32;
-      excl += warp_sum(lane < z ? static_cast<long long>(f & FLAG_VAL) : 0ll);
+    int z = 32 * PER;  // distance of the nearest unpublished flag
+    int p = 32 * PER;  // distance of the nearest inclusive prefix
+#pragma unroll
+    for (int k = PER - 1; k >= 0; --k) {
+      const unsigned nr = __ballot_sync(0xffffffffu, (f[k] >> 62) == 0ull);
+      const unsigned inc = __ballot_sync(0xffffffffu, (f[k] >> 62) == 2ull);
+      if (nr) z = 32 * k + __ffs(nr) - 1;
+      if (inc) p = 32 * k + __ffs(inc) - 1;
+    }
+    if (p < z) {
+      long long s = 0;
+#pragma unroll
+      for (int k = 0; k < PER; ++k)
+        if (lane + 32 * k <= p) s += static_cast<long long>(f[k] & FLAG_VAL);
+      return excl + warp_sum(s);
+    }
+    if (z > 0) {
+      long long s = 0;
+#pragma unroll
+      for (int k = 0; k < PER; ++k)
+        if (lane + 32 * k < z) s += static_cast<long long>(f[k] & FLAG_VAL);
+      excl += warp_sum(s);
       end -= z;
       continue;
     }
-    // nearest predecessor not ready yet: back off, bounded in time
+    // the nearest predecessor has not published yet: back off, bounded in time
     if (++polls == 64) {
       t0 = globaltimer_ns();
     } else if (polls > 64 && (polls & 63) == 0) {
@@ -335,9 +353,9 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
       const bool failed = ld_relaxed_u64(&ws[WS_STATUS]) != 0ull;
       if (__any_sync(0xffffffffu, late || failed)) return -1;
     }
-    if (polls > 8) {
+    if (polls > 4) {
       __nanosleep(sleep_ns);
-      if (sleep_ns < 1024) sleep_ns <<= 1;
+      if (sleep_ns < 512) sleep_ns <<= 1;
     }
   }
 }

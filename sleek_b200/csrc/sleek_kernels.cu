@@ -23,29 +23,108 @@
 namespace sleek {
 
 constexpr int TBUF_BYTES = 16896;  // (4096 + 128) u32 or (2048 + 64) u64, padded layout
+constexpr int ENC_STAGES = 3;
+constexpr int ENC_CW = 8;                    // compute warps
+constexpr int ENC_NT = (ENC_CW + 1) * 32;    // + one control warp
+constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
-struct EncMisc {
-  uint64_t bar[2];
-  long long ticket[2];
-  long long excl;
-  int lnv[SC];
-  int cumw[SC + 1];
-  unsigned rcp[SC];
+struct EncMeta {
+  long long c;     // chunk id, or NO_CHUNK: no more work for this CTA
+  long long excl;  // byte offset of the chunk's payload (or -1 after an error)
+  int osize;
   int csize;
   int comp;
-  int abort;
+  int pad_;
 };
 
-constexpr int ENC_SMEM = 2 * STAGE_BYTES + TBUF_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
+struct EncMisc {
+  uint64_t full[ENC_STAGES];    // TMA landed (tx count)
+  uint64_t empty[ENC_STAGES];   // compute warps done with the stage
+  uint64_t sized[ENC_STAGES];   // compressed size of the stage's chunk known
+  uint64_t placed[ENC_STAGES];  // payload offset of the stage's chunk known
+  EncMeta meta[ENC_STAGES];
+  int lnv[SC];
+  int cumw[SC + 1];             // packed words before each subchunk (u32 words for f32, u64 for f64)
+  unsigned rcp[SC];
+};
 
-template <typename T, bool LOSSY, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_encode(const EncArgs a)
+constexpr int ENC_MINB = 3;
+constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + TBUF_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
+
+// barrier among the compute warps only (named barrier 1)
+__device__ __forceinline__ void cbar()
+{
+  asm volatile("bar.sync 1, %0;" ::"n"(ENC_CW * 32) : "memory");
+}
+
+__device__ __forceinline__ bool cbar_or(bool pred)
+{
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(static_cast<uint32_t>(pred)), "n"(ENC_CW * 32)
+      : "memory");
+  return r != 0;
+}
+
+// Packs subchunk-ordered transformed values into the chunk payload: each lane
+// assembles whole output words (u32 words for 32-bit values, u64 words for
+// 64-bit values) from the values whose bits overlap them.
+template <typename T>
+__device__ __forceinline__ void pack_chunk(const T* tb, uint8_t* stg, const EncMisc& m, int cw, int lane)
+{
+  using V = VT<T>;
+  using W = T;  // output word type: same width as the values
+  constexpr int WB = V::TB;
+  W* const pw = reinterpret_cast<W*>(stg + 32);
+  for (int i = cw; i < SC; i += ENC_CW) {
+    const int ln = m.lnv[i];
+    if (ln == 0) continue;
+    const int words = (V::VPS * ln) / WB;
+    const int base = m.cumw[i];
+    const unsigned rcp = m.rcp[i];
+    const int kb = i * V::VPS;
+    for (int q = lane; q < words; q += 32) {
+      const int start = q * WB;
+      int k = ln > 1 ? static_cast<int>(__umulhi(static_cast<unsigned>(start), rcp)) : start;
+      const int off = k * ln - start;  // in (-ln, 0]
+      if constexpr (WB == 32) {
+        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
+        int n = ln + off;
+        ++k;
+        while (n < 32 && k < V::VPS) {
+          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
+          n += ln;
+          ++k;
+        }
+        pw[base + q] = static_cast<uint32_t>(acc);
+      } else {
+        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
+        int n = ln + off;
+        ++k;
+        while (n < 64 && k < V::VPS) {
+          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
+          n += ln;
+          ++k;
+        }
+        pw[base + q] = acc;
+      }
+    }
+  }
+}
+
+template <typename T, bool LOSSY, int MINB>
+__global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
 {
   using V = VT<T>;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const stage0 = smem;
-  T* const tb = reinterpret_cast<T*>(smem + 2 * STAGE_BYTES);
-  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + 2 * STAGE_BYTES + TBUF_BYTES);
+  T* const tb = reinterpret_cast<T*>(smem + ENC_STAGES * STAGE_BYTES);
+  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + ENC_STAGES * STAGE_BYTES + TBUF_BYTES);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -57,183 +136,225 @@ __global__ void __launch_bounds__(NT, MINB) k_encode(const EncArgs a)
   uint8_t* const data_out = a.out + 8 + 2 * chunks;
   const bool in_aligned = (reinterpret_cast<uintptr_t>(a.in) & 15u) == 0u;
 
-  auto issue = [&](long long c, int stg) {  // thread 0 only
-    const long long base = c * CS;
-    const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-    const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
-    if (tbytes) {
-      mbar_arrive_expect_tx(&m.bar[stg], tbytes);
-      tma_load_1d(stage0 + stg * STAGE_BYTES, a.in + base, tbytes, &m.bar[stg]);
-    } else {
-      mbar_arrive(&m.bar[stg]);
-    }
-  };
-
-  long long next_ticket = 0;
   if (tid == 0) {
-    mbar_init(&m.bar[0], 1);
-    mbar_init(&m.bar[1], 1);
+    for (int s = 0; s < ENC_STAGES; ++s) {
+      mbar_init(&m.full[s], 1);
+      mbar_init(&m.empty[s], 1);
+      mbar_init(&m.sized[s], 1);
+      mbar_init(&m.placed[s], 1);
+    }
     mbar_fence_init();
-    const long long t0 = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
-    next_ticket = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
-    m.ticket[0] = t0;
-    m.abort = 0;
-    if (t0 < chunks) issue(t0, 0);
   }
   __syncthreads();
 
-  for (int it = 0;; ++it) {
-    const int s = it & 1;
-    const long long c = m.ticket[s];
-    if (c >= chunks) break;
-    uint8_t* const stg = stage0 + s * STAGE_BYTES;
-
-    if (tid == 0) {  // prefetch the next ticket's chunk into the other stage
-      const long long t = next_ticket;
-      m.ticket[s ^ 1] = t;
+  if (warp == ENC_CW) {
+    // ===================== control warp: tickets, TMA, look-back =====================
+    long long tk_cur = 0, tk_next = 0, nt = 0;
+    unsigned issued = 0;      // stages with a TMA issued
+    unsigned issued_par = 0;  // parity of the last TMA issued per stage
+    auto issue = [&](long long t, int s, int seq) {  // lane 0
+      EncMeta& me = m.meta[s];
       if (t < chunks) {
-        issue(t, s ^ 1);
-        next_ticket = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
-      }
-    }
-
-    const bool arrived = mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
-    if (__syncthreads_or(!arrived)) {
-      if (tid == 0) set_status(ws, ST_TIMEOUT, c);
-      // let any copy still in flight into this CTA's shared memory land first
-      mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
-      mbar_wait_bounded(&m.bar[s ^ 1], ((it + 1) >> 1) & 1);
-      break;
-    }
-
-    // ---- phase A: transform / quantize, subchunk bit widths ----------------
-    const long long base = c * CS;
-    const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-    const int tbytes = in_aligned ? (osize & ~15) : 0;
-    {
-      T* const sv = reinterpret_cast<T*>(stg);
-      const T* const gin = reinterpret_cast<const T*>(a.in + base);
-      constexpr int PER = V::VPS / 32;
-      for (int i = warp; i < SC; i += NT / 32) {
-        T mx = 0;
-        if (tbytes == CS) {
-#pragma unroll
-          for (int u = 0; u < PER; ++u) {
-            const int k = i * V::VPS + u * 32 + lane;
-            const T e = encode_value<LOSSY>(sv[k], a.q);
-            tb[tpad(k)] = e;
-            mx = e > mx ? e : mx;
-          }
+        const long long base = t * CS;
+        const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+        const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
+        me.c = t;
+        if (tbytes) {
+          mbar_arrive_expect_tx(&m.full[s], tbytes);
+          tma_load_1d(stage0 + s * STAGE_BYTES, a.in + base, tbytes, &m.full[s]);
+          issued |= 1u << s;
+          issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
         } else {
-#pragma unroll
-          for (int u = 0; u < PER; ++u) {
-            const int k = i * V::VPS + u * 32 + lane;
-            const int b = k * static_cast<int>(sizeof(T));
-            T v = 0;
-            if (b < tbytes) {
-              v = sv[k];
-            } else if (b < osize) {
-              v = gin[k];
-              sv[k] = v;  // keep the staged copy complete for a raw store
-            }
-            const T e = encode_value<LOSSY>(v, a.q);  // zero padding is transformed too
-            tb[tpad(k)] = e;
-            mx = e > mx ? e : mx;
-          }
+          issued &= ~(1u << s);
+          mbar_arrive(&m.full[s]);
         }
-        mx = warp_max(mx);
-        if (lane == 0) m.lnv[i] = bit_width(mx);
+      } else {
+        me.c = NO_CHUNK;
+        issued &= ~(1u << s);
+        mbar_arrive(&m.full[s]);
       }
+    };
+    if (lane == 0) {
+      unsigned long long* tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
+      tk_cur = static_cast<long long>(atomicAdd(tick, 1ull));
+      tk_next = static_cast<long long>(atomicAdd(tick, 1ull));
+      nt = static_cast<long long>(atomicAdd(tick, 1ull));
+      issue(tk_cur, 0, 0);
+      issue(tk_next, 1, 1);
     }
-    __syncthreads();
-
-    // ---- widths scan, size decision, publish aggregate ----------------------
-    if (warp == 0) {
-      const int ln = m.lnv[lane];
-      const int wc = ln * V::WPS_PER_LN;
-      int incl = wc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
+    for (int seq = 0;; ++seq) {
+      const int s = seq % ENC_STAGES;
+      const long long c = __shfl_sync(0xffffffffu, tk_cur, 0);
+      if (c >= chunks) break;
+      const bool ok = mbar_wait_bounded(&m.sized[s], (seq / ENC_STAGES) & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, c);
+        break;
       }
-      m.cumw[lane + 1] = incl;
-      m.rcp[lane] = ln > 1 ? static_cast<unsigned>(((1ull << 32) + ln - 1) / ln) : 0u;
-      if (lane == 0) m.cumw[0] = 0;
-      const int W = __shfl_sync(0xffffffffu, incl, 31);
-      const int newsize = 34 + 8 * W;
-      const bool comp = newsize < osize;
-      const int csize = comp ? newsize : osize;
-      if (lane == 0) {
-        m.csize = csize;
-        m.comp = comp;
-        st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
-      }
-    }
-    __syncthreads();
-
-    const int csize = m.csize;
-    const bool comp = m.comp != 0;
-    const int W = m.cumw[SC];
-
-    // ---- look-back (warp 0)  ||  gather-form packing (warps 1..) ------------
-    if (warp == 0) {
+      const int csize = m.meta[s].csize;
       long long excl = 0;
       if (c > 0) {
         excl = lookback(flags, c, 0, ws);
         unsigned err = 0;
         if (excl < 0) err = ST_TIMEOUT;
         else if (excl > c * CS) err = ST_CAPACITY;
-        if (err) {
-          if (lane == 0) set_status(ws, err, c);
-          excl = -1;
-        }
-        // an impossible prefix is replaced by the largest legal one so that
-        // every later chunk still writes inside the output bound
-        if (lane == 0)
+        if (err) excl = -1;
+        if (lane == 0) {
+          if (err) set_status(ws, err, c);
+          // an impossible prefix is replaced by the largest legal one so that
+          // every later chunk still writes inside the output bound
           st_release_u64(&flags[c], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
+        }
       }
       if (lane == 0) {
-        m.excl = excl;
+        m.meta[s].excl = excl;
         if (c == chunks - 1 && excl >= 0) ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
+        mbar_arrive(&m.placed[s]);
       }
-      if (comp) {
-        stg[lane] = static_cast<uint8_t>(m.lnv[lane]);
-        if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 8 * W) = static_cast<int16_t>(osize);
-      }
-    } else if (comp) {
-      uint64_t* const pw = reinterpret_cast<uint64_t*>(stg + 32);
-      for (int g = tid - 32; g < W; g += NT - 32) {
-        int i = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1)
-          if (m.cumw[i + step] <= g) i += step;
-        const int ln = m.lnv[i];
-        const int start = (g - m.cumw[i]) * 64;
-        int k = ln > 1 ? static_cast<int>(__umulhi(static_cast<unsigned>(start), m.rcp[i])) : start;
-        const int off = k * ln - start;  // in (-ln, 0]
-        const int kb = i * V::VPS;
-        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
-        int n = ln + off;
-        ++k;
-        while (n < 64 && k < V::VPS) {
-          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
-          n += ln;
-          ++k;
+      // refill the stage last used by seq - 1 with the chunk of seq + 2
+      const int s2 = (seq + 2) % ENC_STAGES;
+      if (seq >= 1) {
+        const bool ok2 = mbar_wait_bounded(&m.empty[s2], ((seq - 1) / ENC_STAGES) & 1);
+        if (__any_sync(0xffffffffu, !ok2)) {
+          if (lane == 0) set_status(ws, ST_TIMEOUT, c);
+          break;
         }
-        pw[g] = acc;
+      }
+      if (lane == 0) {
+        const long long t = nt;
+        issue(t, s2, seq + 2);
+        if (t < chunks) nt = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
+        tk_cur = tk_next;
+        tk_next = t;
       }
     }
-    __syncthreads();
-
-    // ---- store the chunk at its byte offset ----------------------------------
-    const long long excl = m.excl;
-    if (excl >= 0) {
-      store_shifted<NT>(data_out + excl, stg, csize);
-      if (tid == 0) *reinterpret_cast<uint16_t*>(size_out + 2 * c) = static_cast<uint16_t>(csize);
+    // never leave with a bulk copy still landing in this CTA's shared memory
+    if (lane == 0) {
+      for (int s = 0; s < ENC_STAGES; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
-    fence_proxy_async_smem();  // generic accesses of this stage before the next TMA write
-    __syncthreads();
+  } else {
+    // ===================== compute warps =====================
+    const int cw = warp;
+    int last = -1;        // seq of the last chunk processed, still to be stored
+    bool failed = false;
+    auto store = [&](int sq) {
+      const int sp = sq % ENC_STAGES;
+      const bool ok = mbar_wait_bounded(&m.placed[sp], (sq / ENC_STAGES) & 1);
+      if (cbar_or(!ok)) {
+        if (tid == 0) set_status(ws, ST_TIMEOUT, m.meta[sp].c);
+        return false;
+      }
+      const EncMeta me = m.meta[sp];
+      if (me.excl >= 0) {
+        store_shifted<ENC_CW * 32>(data_out + me.excl, stage0 + sp * STAGE_BYTES, me.csize);
+        if (tid == 0) *reinterpret_cast<uint16_t*>(size_out + 2 * me.c) = static_cast<uint16_t>(me.csize);
+      }
+      return true;
+    };
+
+    for (int seq = 0;; ++seq) {
+      const int s = seq % ENC_STAGES;
+      const bool arrived = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
+      if (cbar_or(!arrived)) {
+        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+        failed = true;
+        break;
+      }
+      const long long c = m.meta[s].c;
+      if (c == NO_CHUNK) break;
+      uint8_t* const stg = stage0 + s * STAGE_BYTES;
+
+      // ---- phase A: transform / quantize, subchunk bit widths ----------------
+      const long long base = c * CS;
+      const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+      const int tbytes = in_aligned ? (osize & ~15) : 0;
+      {
+        T* const sv = reinterpret_cast<T*>(stg);
+        const T* const gin = reinterpret_cast<const T*>(a.in + base);
+        constexpr int PER = V::VPS / 32;
+        for (int i = cw; i < SC; i += ENC_CW) {
+          T mx = 0;
+          if (tbytes == CS) {
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+              const int k = i * V::VPS + u * 32 + lane;
+              const T e = encode_value<LOSSY>(sv[k], a.q);
+              tb[tpad(k)] = e;
+              mx = e > mx ? e : mx;
+            }
+          } else {
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+              const int k = i * V::VPS + u * 32 + lane;
+              const int b = k * static_cast<int>(sizeof(T));
+              T v = 0;
+              if (b < tbytes) {
+                v = sv[k];
+              } else if (b < osize) {
+                v = gin[k];
+                sv[k] = v;  // keep the staged copy complete for a raw store
+              }
+              const T e = encode_value<LOSSY>(v, a.q);  // zero padding is transformed too
+              tb[tpad(k)] = e;
+              mx = e > mx ? e : mx;
+            }
+          }
+          mx = warp_max(mx);
+          if (lane == 0) m.lnv[i] = bit_width(mx);
+        }
+      }
+      cbar();
+
+      // ---- widths scan, size decision, publish the aggregate -----------------
+      if (cw == 0) {
+        const int ln = m.lnv[lane];
+        const int wc = (V::VPS * ln) / V::TB;  // output words of this subchunk
+        int incl = wc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        m.cumw[lane + 1] = incl;
+        m.rcp[lane] = ln > 1 ? static_cast<unsigned>(((1ull << 32) + ln - 1) / ln) : 0u;
+        if (lane == 0) m.cumw[0] = 0;
+        const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+        const int newsize = 34 + wtot * static_cast<int>(sizeof(T));
+        const bool comp = newsize < osize;
+        const int csize = comp ? newsize : osize;
+        if (lane == 0) {
+          m.meta[s].osize = osize;
+          m.meta[s].csize = csize;
+          m.meta[s].comp = comp;
+          st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+        }
+      }
+      cbar();
+      if (tid == 0) mbar_arrive(&m.sized[s]);
+
+      // ---- pack this chunk, then store the previous one ----------------------
+      if (m.meta[s].comp) {
+        pack_chunk<T>(tb, stg, m, cw, lane);
+        if (cw == 0) {
+          stg[lane] = static_cast<uint8_t>(m.lnv[lane]);
+          if (lane == 0)
+            *reinterpret_cast<int16_t*>(stg + 32 + m.cumw[SC] * static_cast<int>(sizeof(T))) =
+                static_cast<int16_t>(osize);
+        }
+      }
+      if (last >= 0) {
+        if (!store(last)) {
+          failed = true;
+          break;
+        }
+      }
+      fence_proxy_async_smem();  // generic accesses of the stage before its next TMA write
+      cbar();
+      if (last >= 0 && tid == 0) mbar_arrive(&m.empty[last % ENC_STAGES]);
+      last = seq;
+    }
+    if (!failed && last >= 0) store(last);
   }
 
   // ---- epilogue: the last CTA out writes the header and the stream size ------
@@ -519,12 +640,11 @@ static cudaError_t ensure_smem_attr(K k, int bytes, unsigned long long* done_mas
 template <typename T, bool LOSSY>
 static cudaError_t launch_encode_t(const EncArgs& a, int grid, cudaStream_t st)
 {
-  constexpr int NT = 256, MINB = 4;
-  auto k = k_encode<T, LOSSY, NT, MINB>;
+  auto k = k_encode<T, LOSSY, ENC_MINB>;
   static unsigned long long attr = 0;
   cudaError_t e = ensure_smem_attr(k, ENC_SMEM, &attr);
   if (e != cudaSuccess) return e;
-  k<<<grid, NT, ENC_SMEM, st>>>(a);
+  k<<<grid, ENC_NT, ENC_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -544,7 +664,7 @@ template <typename T, bool LOSSY>
 static int occupancy_t(bool enc)
 {
   int n = 0;
-  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<T, LOSSY, 256, 4>, 256, ENC_SMEM);
+  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<T, LOSSY, ENC_MINB>, ENC_NT, ENC_SMEM);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decode<T, LOSSY, 256, 4>, 256, DEC_SMEM);
   return n;
 }
@@ -566,20 +686,20 @@ int blocks_per_sm(int width, bool lossy, bool enc)
   // the smem attribute must be set before the occupancy query counts dynamic smem
   if (width == 4) {
     if (lossy) {
-      cudaFuncSetAttribute(k_encode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+      cudaFuncSetAttribute(k_encode<uint32_t, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
       cudaFuncSetAttribute(k_decode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
       return occupancy_t<uint32_t, true>(enc);
     }
-    cudaFuncSetAttribute(k_encode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_encode<uint32_t, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
     cudaFuncSetAttribute(k_decode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
     return occupancy_t<uint32_t, false>(enc);
   }
   if (lossy) {
-    cudaFuncSetAttribute(k_encode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_encode<uint64_t, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
     cudaFuncSetAttribute(k_decode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
     return occupancy_t<uint64_t, true>(enc);
   }
-  cudaFuncSetAttribute(k_encode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+  cudaFuncSetAttribute(k_encode<uint64_t, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
   cudaFuncSetAttribute(k_decode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
   return occupancy_t<uint64_t, false>(enc);
 }
