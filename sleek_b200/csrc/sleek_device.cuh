@@ -282,6 +282,18 @@ __device__ __forceinline__ uint64_t warp_max(uint64_t v)
   return v;
 }
 
+// bit width of the largest value held by the warp, from the OR of all values
+__device__ __forceinline__ int warp_bit_width(uint32_t v)
+{
+  return bit_width(__reduce_or_sync(0xffffffffu, v));
+}
+__device__ __forceinline__ int warp_bit_width(uint64_t v)
+{
+  const uint32_t hi = __reduce_or_sync(0xffffffffu, static_cast<uint32_t>(v >> 32));
+  const uint32_t lo = __reduce_or_sync(0xffffffffu, static_cast<uint32_t>(v));
+  return hi ? 64 - __clz(hi) : bit_width(lo);
+}
+
 __device__ __forceinline__ long long warp_sum(long long v)
 {
 #pragma unroll

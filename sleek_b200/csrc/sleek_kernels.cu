@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
 
   if (warp == ENC_CW) {
     // ===================== control warp: tickets, TMA, look-back =====================
-    long long tk_cur = 0, tk_next = 0, nt = 0;
+    long long tk_cur = 0, tk_next = 0;
     unsigned issued = 0;      // stages with a TMA issued
     unsigned issued_par = 0;  // parity of the last TMA issued per stage
     auto issue = [&](long long t, int s, int seq) {  // lane 0
@@ -174,12 +174,14 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         mbar_arrive(&m.full[s]);
       }
     };
+    // Tickets are taken just before their chunk's copy is issued, never earlier:
+    // a ticket held long before its chunk is processed makes every later chunk's
+    // look-back wait for it.
+    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
     if (lane == 0) {
-      unsigned long long* tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
       tk_cur = static_cast<long long>(atomicAdd(tick, 1ull));
-      tk_next = static_cast<long long>(atomicAdd(tick, 1ull));
-      nt = static_cast<long long>(atomicAdd(tick, 1ull));
       issue(tk_cur, 0, 0);
+      tk_next = tk_cur < chunks ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
       issue(tk_next, 1, 1);
     }
     for (int seq = 0;; ++seq) {
@@ -221,9 +223,8 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         }
       }
       if (lane == 0) {
-        const long long t = nt;
+        const long long t = tk_next < chunks ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
         issue(t, s2, seq + 2);
-        if (t < chunks) nt = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
         tk_cur = tk_next;
         tk_next = t;
       }
@@ -274,14 +275,14 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         const T* const gin = reinterpret_cast<const T*>(a.in + base);
         constexpr int PER = V::VPS / 32;
         for (int i = cw; i < SC; i += ENC_CW) {
-          T mx = 0;
+          T mx = 0;  // OR of the subchunk's values: same highest set bit as their max
           if (tbytes == CS) {
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
               const int k = i * V::VPS + u * 32 + lane;
               const T e = encode_value<LOSSY>(sv[k], a.q);
               tb[tpad(k)] = e;
-              mx = e > mx ? e : mx;
+              mx |= e;
             }
           } else {
 #pragma unroll
@@ -297,11 +298,11 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
               }
               const T e = encode_value<LOSSY>(v, a.q);  // zero padding is transformed too
               tb[tpad(k)] = e;
-              mx = e > mx ? e : mx;
+              mx |= e;
             }
           }
-          mx = warp_max(mx);
-          if (lane == 0) m.lnv[i] = bit_width(mx);
+          const int w = warp_bit_width(mx);
+          if (lane == 0) m.lnv[i] = w;
         }
       }
       cbar();
