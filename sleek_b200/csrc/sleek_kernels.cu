@@ -22,10 +22,10 @@
 
 namespace sleek {
 
-constexpr int TBUF_BYTES = 16896;  // (4096 + 128) u32 or (2048 + 64) u64, padded layout
-constexpr int ENC_STAGES = 3;
+constexpr int ENC_STAGES = 4;
 constexpr int ENC_CW = 8;                    // compute warps
 constexpr int ENC_NT = (ENC_CW + 1) * 32;    // + one control warp
+constexpr int ENC_MINB = 3;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
 struct EncMeta {
@@ -38,18 +38,15 @@ struct EncMeta {
 };
 
 struct EncMisc {
-  uint64_t full[ENC_STAGES];    // TMA landed (tx count)
+  uint64_t full[ENC_STAGES];    // chunk bytes landed (TMA tx count)
   uint64_t empty[ENC_STAGES];   // compute warps done with the stage
   uint64_t sized[ENC_STAGES];   // compressed size of the stage's chunk known
   uint64_t placed[ENC_STAGES];  // payload offset of the stage's chunk known
   EncMeta meta[ENC_STAGES];
   int lnv[SC];
-  int cumw[SC + 1];             // packed words before each subchunk (u32 words for f32, u64 for f64)
-  unsigned rcp[SC];
 };
 
-constexpr int ENC_MINB = 3;
-constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + TBUF_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
+constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
 
 // barrier among the compute warps only (named barrier 1)
 __device__ __forceinline__ void cbar()
@@ -71,49 +68,93 @@ __device__ __forceinline__ bool cbar_or(bool pred)
   return r != 0;
 }
 
-// Packs subchunk-ordered transformed values into the chunk payload: each lane
-// assembles whole output words (u32 words for 32-bit values, u64 words for
-// 64-bit values) from the values whose bits overlap them.
+// Appends the bits of the stream in order and hands out each completed 32-bit
+// word: the first one is kept (its low bits belong to the previous lane), the
+// others are stored at consecutive word slots.
+struct WordSink {
+  uint32_t* dst;  // slot of the lane's first word
+  uint32_t first;
+  int j;
+  __device__ __forceinline__ void emit(uint32_t w)
+  {
+    if (j == 0) first = w;
+    else dst[j] = w;
+    ++j;
+  }
+};
+
+// Packs one subchunk whose transformed values sit in registers: lane L holds
+// values P*L .. P*L+P-1 and writes the bit run [P*L*ln, P*(L+1)*ln) of the
+// subchunk's packed bits (LSB-first, 32-bit little-endian words at `pw`).
 template <typename T>
-__device__ __forceinline__ void pack_chunk(const T* tb, uint8_t* stg, const EncMisc& m, int cw, int lane)
+__device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)[16 / sizeof(T)], int lane)
 {
-  using V = VT<T>;
-  using W = T;  // output word type: same width as the values
-  constexpr int WB = V::TB;
-  W* const pw = reinterpret_cast<W*>(stg + 32);
-  for (int i = cw; i < SC; i += ENC_CW) {
-    const int ln = m.lnv[i];
-    if (ln == 0) continue;
-    const int words = (V::VPS * ln) / WB;
-    const int base = m.cumw[i];
-    const unsigned rcp = m.rcp[i];
-    const int kb = i * V::VPS;
-    for (int q = lane; q < words; q += 32) {
-      const int start = q * WB;
-      int k = ln > 1 ? static_cast<int>(__umulhi(static_cast<unsigned>(start), rcp)) : start;
-      const int off = k * ln - start;  // in (-ln, 0]
-      if constexpr (WB == 32) {
-        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
-        int n = ln + off;
-        ++k;
-        while (n < 32 && k < V::VPS) {
-          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
-          n += ln;
-          ++k;
-        }
-        pw[base + q] = static_cast<uint32_t>(acc);
+  constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane
+  constexpr int TB = 8 * static_cast<int>(sizeof(T));
+  if (ln == 0) return;
+  if (ln == TB) {  // verbatim: the lane's 16 bytes in place
+    uint32_t* d = pw + 4 * lane;
+    if constexpr (sizeof(T) == 4) {
+      if ((reinterpret_cast<uintptr_t>(d) & 15u) == 0u) {
+        *reinterpret_cast<uint4*>(d) = make_uint4(v[0], v[1], v[2], v[3]);
       } else {
-        uint64_t acc = static_cast<uint64_t>(tb[tpad(kb + k)]) >> (-off);
-        int n = ln + off;
-        ++k;
-        while (n < 64 && k < V::VPS) {
-          acc |= static_cast<uint64_t>(tb[tpad(kb + k)]) << n;
-          n += ln;
-          ++k;
+        d[0] = v[0]; d[1] = v[1]; d[2] = v[2]; d[3] = v[3];
+      }
+    } else {
+      reinterpret_cast<uint2*>(d)[0] = make_uint2(static_cast<uint32_t>(v[0]), static_cast<uint32_t>(v[0] >> 32));
+      reinterpret_cast<uint2*>(d)[1] = make_uint2(static_cast<uint32_t>(v[1]), static_cast<uint32_t>(v[1] >> 32));
+    }
+    return;
+  }
+  const int R = P * ln;  // bits of the lane's run
+  const int rs = lane * R;
+  const int w0 = rs >> 5;
+  const int s = rs & 31;
+  if (R >= 32) {
+    // each word holds bits of at most two adjacent lanes: exchange one partial word
+    WordSink out{pw + w0, 0u, 0};
+    uint64_t acc = 0;
+    int n = s;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      if constexpr (sizeof(T) == 4) {
+        acc |= static_cast<uint64_t>(v[k]) << n;
+        n += ln;
+        if (n >= 32) {
+          out.emit(static_cast<uint32_t>(acc));
+          acc >>= 32;
+          n -= 32;
         }
-        pw[base + q] = acc;
+      } else {
+        uint64_t lo = acc | (v[k] << n);
+        const uint32_t hi = n ? static_cast<uint32_t>(v[k] >> (64 - n)) : 0u;
+        n += ln;
+        if (n >= 32) {
+          out.emit(static_cast<uint32_t>(lo));
+          lo = (lo >> 32) | (static_cast<uint64_t>(hi) << 32);
+          n -= 32;
+          if (n >= 32) {
+            out.emit(static_cast<uint32_t>(lo));
+            lo >>= 32;
+            n -= 32;
+          }
+        }
+        acc = lo;
       }
     }
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, static_cast<uint32_t>(acc), 1);
+    pw[w0] = s ? (out.first | prev) : out.first;
+  } else {
+    // short runs: several lanes share a word; clear the words, then OR in
+    const int words = (32 * P * ln) >> 5;
+    for (int q = lane; q < words; q += 32) pw[q] = 0u;
+    __syncwarp();
+    uint32_t run = 0;
+#pragma unroll
+    for (int k = 0; k < P; ++k) run |= static_cast<uint32_t>(v[k]) << (k * ln);
+    const uint64_t sh = static_cast<uint64_t>(run) << s;
+    if (static_cast<uint32_t>(sh)) atomicOr(&pw[w0], static_cast<uint32_t>(sh));
+    if (static_cast<uint32_t>(sh >> 32)) atomicOr(&pw[w0 + 1], static_cast<uint32_t>(sh >> 32));
   }
 }
 
@@ -121,10 +162,11 @@ template <typename T, bool LOSSY, int MINB>
 __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
 {
   using V = VT<T>;
+  constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane per subchunk
+  constexpr int SPW = SC / ENC_CW;                      // subchunks per compute warp
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const stage0 = smem;
-  T* const tb = reinterpret_cast<T*>(smem + ENC_STAGES * STAGE_BYTES);
-  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + ENC_STAGES * STAGE_BYTES + TBUF_BYTES);
+  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + ENC_STAGES * STAGE_BYTES);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -150,8 +192,8 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
   if (warp == ENC_CW) {
     // ===================== control warp: tickets, TMA, look-back =====================
     long long tk_cur = 0, tk_next = 0;
-    unsigned issued = 0;      // stages with a TMA issued
-    unsigned issued_par = 0;  // parity of the last TMA issued per stage
+    unsigned issued = 0;      // stages whose last use was a TMA copy
+    unsigned issued_par = 0;  // parity of that use
     auto issue = [&](long long t, int s, int seq) {  // lane 0
       EncMeta& me = m.meta[s];
       if (t < chunks) {
@@ -164,15 +206,13 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
           tma_load_1d(stage0 + s * STAGE_BYTES, a.in + base, tbytes, &m.full[s]);
           issued |= 1u << s;
           issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
-        } else {
-          issued &= ~(1u << s);
-          mbar_arrive(&m.full[s]);
+          return;
         }
       } else {
         me.c = NO_CHUNK;
-        issued &= ~(1u << s);
-        mbar_arrive(&m.full[s]);
       }
+      issued &= ~(1u << s);
+      mbar_arrive(&m.full[s]);
     };
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
@@ -213,10 +253,10 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         if (c == chunks - 1 && excl >= 0) ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
         mbar_arrive(&m.placed[s]);
       }
-      // refill the stage last used by seq - 1 with the chunk of seq + 2
+      // refill the stage last used by seq - 2 with the chunk of seq + 2
       const int s2 = (seq + 2) % ENC_STAGES;
-      if (seq >= 1) {
-        const bool ok2 = mbar_wait_bounded(&m.empty[s2], ((seq - 1) / ENC_STAGES) & 1);
+      if (seq >= 2) {
+        const bool ok2 = mbar_wait_bounded(&m.empty[s2], ((seq - 2) / ENC_STAGES) & 1);
         if (__any_sync(0xffffffffu, !ok2)) {
           if (lane == 0) set_status(ws, ST_TIMEOUT, c);
           break;
@@ -237,125 +277,127 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
   } else {
     // ===================== compute warps =====================
     const int cw = warp;
-    int last = -1;        // seq of the last chunk processed, still to be stored
-    bool failed = false;
-    auto store = [&](int sq) {
+    auto store = [&](int sq) {  // all compute threads; placed[] already observed
       const int sp = sq % ENC_STAGES;
-      const bool ok = mbar_wait_bounded(&m.placed[sp], (sq / ENC_STAGES) & 1);
-      if (cbar_or(!ok)) {
-        if (tid == 0) set_status(ws, ST_TIMEOUT, m.meta[sp].c);
-        return false;
-      }
       const EncMeta me = m.meta[sp];
       if (me.excl >= 0) {
         store_shifted<ENC_CW * 32>(data_out + me.excl, stage0 + sp * STAGE_BYTES, me.csize);
         if (tid == 0) *reinterpret_cast<uint16_t*>(size_out + 2 * me.c) = static_cast<uint16_t>(me.csize);
       }
-      return true;
     };
 
-    for (int seq = 0;; ++seq) {
+    int seq = 0;
+    bool failed = false;
+    for (;; ++seq) {
       const int s = seq % ENC_STAGES;
-      const bool arrived = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
-      if (cbar_or(!arrived)) {
+      bool ok = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
+      if (seq >= 2) ok = mbar_wait_bounded(&m.placed[(seq - 2) % ENC_STAGES], ((seq - 2) / ENC_STAGES) & 1) && ok;
+      if (cbar_or(!ok)) {
         if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
         failed = true;
         break;
       }
+      // every compute warp is past the store of seq - 3: its stage can be refilled
+      if (seq >= 3 && tid == 0) mbar_arrive(&m.empty[(seq - 3) % ENC_STAGES]);
       const long long c = m.meta[s].c;
       if (c == NO_CHUNK) break;
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
 
-      // ---- phase A: transform / quantize, subchunk bit widths ----------------
+      // ---- phase A: values into registers, transform / quantize, bit widths ----
       const long long base = c * CS;
       const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
       const int tbytes = in_aligned ? (osize & ~15) : 0;
-      {
-        T* const sv = reinterpret_cast<T*>(stg);
-        const T* const gin = reinterpret_cast<const T*>(a.in + base);
-        constexpr int PER = V::VPS / 32;
-        for (int i = cw; i < SC; i += ENC_CW) {
-          T mx = 0;  // OR of the subchunk's values: same highest set bit as their max
-          if (tbytes == CS) {
+      T vals[SPW][P];
 #pragma unroll
-            for (int u = 0; u < PER; ++u) {
-              const int k = i * V::VPS + u * 32 + lane;
-              const T e = encode_value<LOSSY>(sv[k], a.q);
-              tb[tpad(k)] = e;
-              mx |= e;
-            }
+      for (int u = 0; u < SPW; ++u) {
+        const int i = cw + u * ENC_CW;
+        const int k0 = i * V::VPS + lane * P;  // first value of this lane in the chunk
+        if (tbytes == CS) {
+          const uint4 q = *reinterpret_cast<const uint4*>(stg + k0 * sizeof(T));
+          if constexpr (sizeof(T) == 4) {
+            vals[u][0] = q.x; vals[u][1] = q.y; vals[u][2] = q.z; vals[u][3] = q.w;
           } else {
-#pragma unroll
-            for (int u = 0; u < PER; ++u) {
-              const int k = i * V::VPS + u * 32 + lane;
-              const int b = k * static_cast<int>(sizeof(T));
-              T v = 0;
-              if (b < tbytes) {
-                v = sv[k];
-              } else if (b < osize) {
-                v = gin[k];
-                sv[k] = v;  // keep the staged copy complete for a raw store
-              }
-              const T e = encode_value<LOSSY>(v, a.q);  // zero padding is transformed too
-              tb[tpad(k)] = e;
-              mx |= e;
-            }
+            vals[u][0] = (static_cast<uint64_t>(q.y) << 32) | q.x;
+            vals[u][1] = (static_cast<uint64_t>(q.w) << 32) | q.z;
           }
-          const int w = warp_bit_width(mx);
-          if (lane == 0) m.lnv[i] = w;
-        }
-      }
-      cbar();
-
-      // ---- widths scan, size decision, publish the aggregate -----------------
-      if (cw == 0) {
-        const int ln = m.lnv[lane];
-        const int wc = (V::VPS * ln) / V::TB;  // output words of this subchunk
-        int incl = wc;
+        } else {
+          T* const sv = reinterpret_cast<T*>(stg);
+          const T* const gin = reinterpret_cast<const T*>(a.in + base);
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += t;
+          for (int p = 0; p < P; ++p) {
+            const int k = k0 + p;
+            const int b = k * static_cast<int>(sizeof(T));
+            T x = 0;
+            if (b < tbytes) {
+              x = sv[k];
+            } else if (b < osize) {
+              x = gin[k];
+              sv[k] = x;  // keep the staged copy complete for a raw store
+            }
+            vals[u][p] = x;  // zero padding is transformed too
+          }
         }
-        m.cumw[lane + 1] = incl;
-        m.rcp[lane] = ln > 1 ? static_cast<unsigned>(((1ull << 32) + ln - 1) / ln) : 0u;
-        if (lane == 0) m.cumw[0] = 0;
-        const int wtot = __shfl_sync(0xffffffffu, incl, 31);
-        const int newsize = 34 + wtot * static_cast<int>(sizeof(T));
-        const bool comp = newsize < osize;
-        const int csize = comp ? newsize : osize;
-        if (lane == 0) {
-          m.meta[s].osize = osize;
-          m.meta[s].csize = csize;
-          m.meta[s].comp = comp;
-          st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+        T orv = 0;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          vals[u][p] = encode_value<LOSSY>(vals[u][p], a.q);
+          orv |= vals[u][p];
         }
+        const int w = warp_bit_width(orv);
+        if (lane == 0) m.lnv[i] = w;
       }
       cbar();
-      if (tid == 0) mbar_arrive(&m.sized[s]);
 
-      // ---- pack this chunk, then store the previous one ----------------------
-      if (m.meta[s].comp) {
-        pack_chunk<T>(tb, stg, m, cw, lane);
+      // ---- widths scan (every warp, redundantly), size decision ---------------
+      const int ln_l = m.lnv[lane];
+      const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
+      int incl = wc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+      const int newsize = 34 + 4 * wtot;
+      const bool comp = newsize < osize;
+      const int csize = comp ? newsize : osize;
+      if (tid == 0) {
+        m.meta[s].osize = osize;
+        m.meta[s].csize = csize;
+        m.meta[s].comp = comp;
+        st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+        mbar_arrive(&m.sized[s]);
+      }
+
+      // ---- pack this chunk from registers --------------------------------------
+      if (comp) {
+        uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
+#pragma unroll
+        for (int u = 0; u < SPW; ++u) {
+          const int i = cw + u * ENC_CW;
+          const int wbase = __shfl_sync(0xffffffffu, incl - wc, i);
+          const int ln = __shfl_sync(0xffffffffu, ln_l, i);
+          pack_subchunk<T>(pw + wbase, ln, vals[u], lane);
+        }
         if (cw == 0) {
-          stg[lane] = static_cast<uint8_t>(m.lnv[lane]);
-          if (lane == 0)
-            *reinterpret_cast<int16_t*>(stg + 32 + m.cumw[SC] * static_cast<int>(sizeof(T))) =
-                static_cast<int16_t>(osize);
+          stg[lane] = static_cast<uint8_t>(ln_l);
+          if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
         }
       }
-      if (last >= 0) {
-        if (!store(last)) {
-          failed = true;
-          break;
-        }
-      }
-      fence_proxy_async_smem();  // generic accesses of the stage before its next TMA write
-      cbar();
-      if (last >= 0 && tid == 0) mbar_arrive(&m.empty[last % ENC_STAGES]);
-      last = seq;
+
+      // ---- store the chunk of seq - 2 (its offset is known) ---------------------
+      if (seq >= 2) store(seq - 2);
+      fence_proxy_async_smem();  // generic accesses of this iteration before later TMA writes
     }
-    if (!failed && last >= 0) store(last);
+    if (!failed) {
+      // drain: chunks seq - 2 (placed already observed) and seq - 1
+      if (seq >= 2) store(seq - 2);
+      if (seq >= 1) {
+        const bool ok = mbar_wait_bounded(&m.placed[(seq - 1) % ENC_STAGES], ((seq - 1) / ENC_STAGES) & 1);
+        if (!cbar_or(!ok)) store(seq - 1);
+        else if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+      }
+    }
   }
 
   // ---- epilogue: the last CTA out writes the header and the stream size ------
