@@ -134,6 +134,13 @@ __device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v)
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Flags carry their own value, so publishing one needs no ordering against the
+// thread's earlier stores (a release would wait for the chunk stores in flight).
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v)
+{
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p)
 {
   uint64_t v;

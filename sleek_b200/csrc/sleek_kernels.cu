@@ -24,7 +24,7 @@ namespace sleek {
 
 constexpr int ENC_STAGES = 4;
 constexpr int ENC_CW = 8;                    // compute warps
-constexpr int ENC_NT = (ENC_CW + 1) * 32;    // + one control warp
+constexpr int ENC_NT = (ENC_CW + 2) * 32;    // + a producer warp and a scanner warp
 constexpr int ENC_MINB = 3;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
@@ -39,7 +39,7 @@ struct EncMeta {
 
 struct EncMisc {
   uint64_t full[ENC_STAGES];    // chunk bytes landed (TMA tx count)
-  uint64_t empty[ENC_STAGES];   // compute warps done with the stage
+  uint64_t empty[ENC_STAGES];   // go-ahead for the stage's next copy (its previous chunk is stored)
   uint64_t sized[ENC_STAGES];   // compressed size of the stage's chunk known
   uint64_t placed[ENC_STAGES];  // payload offset of the stage's chunk known
   EncMeta meta[ENC_STAGES];
@@ -190,45 +190,66 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
   __syncthreads();
 
   if (warp == ENC_CW) {
-    // ===================== control warp: tickets, TMA, look-back =====================
-    long long tk_cur = 0, tk_next = 0;
-    unsigned issued = 0;      // stages whose last use was a TMA copy
-    unsigned issued_par = 0;  // parity of that use
-    auto issue = [&](long long t, int s, int seq) {  // lane 0
-      EncMeta& me = m.meta[s];
-      if (t < chunks) {
-        const long long base = t * CS;
-        const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-        const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
-        me.c = t;
-        if (tbytes) {
-          mbar_arrive_expect_tx(&m.full[s], tbytes);
-          tma_load_1d(stage0 + s * STAGE_BYTES, a.in + base, tbytes, &m.full[s]);
-          issued |= 1u << s;
-          issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
-          return;
-        }
-      } else {
-        me.c = NO_CHUNK;
-      }
-      issued &= ~(1u << s);
-      mbar_arrive(&m.full[s]);
-    };
+    // ===================== producer warp: tickets and TMA copies =====================
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
     // look-back wait for it.
-    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
     if (lane == 0) {
-      tk_cur = static_cast<long long>(atomicAdd(tick, 1ull));
-      issue(tk_cur, 0, 0);
-      tk_next = tk_cur < chunks ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
-      issue(tk_next, 1, 1);
+      unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
+      unsigned issued = 0;      // stages whose last use was a TMA copy
+      unsigned issued_par = 0;  // parity of that use
+      bool more = true;
+      for (int seq = 0;; ++seq) {
+        const int s = seq % ENC_STAGES;
+        // From seq 2 on, the copy for chunk seq is issued when the compute warps
+        // start chunk seq - 1: one chunk of lookahead, and the stage's previous
+        // chunk (seq - 4) has been stored by then.
+        if (seq >= 2) {
+          if (!mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1)) {
+            set_status(ws, ST_TIMEOUT, -1);
+            break;
+          }
+        }
+        const long long t = more ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
+        EncMeta& me = m.meta[s];
+        bool copy = false;
+        if (t < chunks) {
+          const long long base = t * CS;
+          const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+          const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
+          me.c = t;
+          if (tbytes) {
+            mbar_arrive_expect_tx(&m.full[s], tbytes);
+            tma_load_1d(stage0 + s * STAGE_BYTES, a.in + base, tbytes, &m.full[s]);
+            copy = true;
+          }
+        } else {
+          me.c = NO_CHUNK;
+          more = false;
+        }
+        if (copy) {
+          issued |= 1u << s;
+          issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
+        } else {
+          issued &= ~(1u << s);
+          mbar_arrive(&m.full[s]);
+        }
+        if (!more) break;
+      }
+      // never leave with a bulk copy still landing in this CTA's shared memory
+      for (int s = 0; s < ENC_STAGES; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
+  } else if (warp == ENC_CW + 1) {
+    // ===================== scanner warp: decoupled look-back =====================
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      const long long c = __shfl_sync(0xffffffffu, tk_cur, 0);
-      if (c >= chunks) break;
-      const bool ok = mbar_wait_bounded(&m.sized[s], (seq / ENC_STAGES) & 1);
+      const uint32_t par = (seq / ENC_STAGES) & 1;
+      bool ok = mbar_wait_bounded(&m.full[s], par);
+      if (__any_sync(0xffffffffu, !ok)) break;  // the compute warps report it
+      const long long c = m.meta[s].c;
+      if (c == NO_CHUNK) break;
+      ok = mbar_wait_bounded(&m.sized[s], par);
       if (__any_sync(0xffffffffu, !ok)) {
         if (lane == 0) set_status(ws, ST_TIMEOUT, c);
         break;
@@ -245,7 +266,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
           if (err) set_status(ws, err, c);
           // an impossible prefix is replaced by the largest legal one so that
           // every later chunk still writes inside the output bound
-          st_release_u64(&flags[c], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
+          st_relaxed_u64(&flags[c], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
         }
       }
       if (lane == 0) {
@@ -253,26 +274,6 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         if (c == chunks - 1 && excl >= 0) ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
         mbar_arrive(&m.placed[s]);
       }
-      // refill the stage last used by seq - 2 with the chunk of seq + 2
-      const int s2 = (seq + 2) % ENC_STAGES;
-      if (seq >= 2) {
-        const bool ok2 = mbar_wait_bounded(&m.empty[s2], ((seq - 2) / ENC_STAGES) & 1);
-        if (__any_sync(0xffffffffu, !ok2)) {
-          if (lane == 0) set_status(ws, ST_TIMEOUT, c);
-          break;
-        }
-      }
-      if (lane == 0) {
-        const long long t = tk_next < chunks ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
-        issue(t, s2, seq + 2);
-        tk_cur = tk_next;
-        tk_next = t;
-      }
-    }
-    // never leave with a bulk copy still landing in this CTA's shared memory
-    if (lane == 0) {
-      for (int s = 0; s < ENC_STAGES; ++s)
-        if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
   } else {
     // ===================== compute warps =====================
@@ -297,8 +298,9 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         failed = true;
         break;
       }
-      // every compute warp is past the store of seq - 3: its stage can be refilled
-      if (seq >= 3 && tid == 0) mbar_arrive(&m.empty[(seq - 3) % ENC_STAGES]);
+      // start of chunk seq: the producer may copy chunk seq + 1 into the stage of
+      // seq - 3, whose store every compute warp has finished
+      if (seq >= 1 && tid == 0) mbar_arrive(&m.empty[(seq + 1) % ENC_STAGES]);
       const long long c = m.meta[s].c;
       if (c == NO_CHUNK) break;
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
         m.meta[s].osize = osize;
         m.meta[s].csize = csize;
         m.meta[s].comp = comp;
-        st_release_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+        st_relaxed_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
         mbar_arrive(&m.sized[s]);
       }
 
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       s2 = warp_sum(s2);
       b2 = __any_sync(0xffffffffu, b2);
       if (b2 && lane == 0) set_status(ws, ST_CORRUPT, c0);
-      if (lane == 0) st_release_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
+      if (lane == 0) st_relaxed_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
       long long excl = 0;
       if (vb > 0) {
         excl = lookback(flags, vb, 0, ws);
@@ -525,7 +527,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
           if (lane == 0) set_status(ws, ST_TIMEOUT, c0);
         }
         if (lane == 0)
-          st_release_u64(&flags[vb], FLAG_INC | (static_cast<uint64_t>(excl >= 0 ? excl + s2 : 0) & FLAG_VAL));
+          st_relaxed_u64(&flags[vb], FLAG_INC | (static_cast<uint64_t>(excl >= 0 ? excl + s2 : 0) & FLAG_VAL));
       }
       if (lane == 0) m.excl = b2 ? -1 : excl;
     }
