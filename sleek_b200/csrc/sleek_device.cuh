@@ -84,15 +84,18 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Tests the phase with the given parity; a thread whose phase is not complete
+// is suspended until it completes (or about 0.5 ms pass), so waiting warps do
+// not spin on issue slots.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(500000u)
       : "memory");
   return ok != 0;
 }
@@ -171,14 +174,23 @@ __device__ __forceinline__ uint32_t fwd(uint32_t v)
   return (v << 1) ^ static_cast<uint32_t>(static_cast<int32_t>(v) >> 31);
 }
 
+// 64-bit lossless forward transform on 32-bit halves: the exponent test and
+// both subtractions touch only the high word (no borrow crosses into the low
+// word), the rotate and the final shift are funnel shifts.
 __device__ __forceinline__ uint64_t fwd(uint64_t v)
 {
-  v = (v << 1) | (v >> 63);
-  if (v & 0xffe0000000000000ull) {
-    v -= 0x8000000000000000ull;
-    if (((v & 0xffe0000000000000ull) == 0ull) | (v >= 0x8000000000000000ull)) v -= 0x0020000000000000ull;
+  const uint32_t h = static_cast<uint32_t>(v >> 32);
+  const uint32_t l = static_cast<uint32_t>(v);
+  uint32_t nh = __funnelshift_l(l, h, 1);        // rotate left by 1
+  const uint32_t nl = __funnelshift_l(h, l, 1);
+  if (nh & 0xffe00000u) {
+    nh -= 0x80000000u;
+    if (((nh & 0xffe00000u) == 0u) | (nh >= 0x80000000u)) nh -= 0x00200000u;
   }
-  return (v << 1) ^ static_cast<uint64_t>(static_cast<int64_t>(v) >> 63);
+  const uint32_t sg = static_cast<uint32_t>(static_cast<int32_t>(nh) >> 31);
+  const uint32_t oh = __funnelshift_l(nl, nh, 1) ^ sg;  // (v << 1) ^ (v >> 63 arithmetic)
+  const uint32_t ol = (nl << 1) ^ sg;
+  return (static_cast<uint64_t>(oh) << 32) | ol;
 }
 
 __device__ __forceinline__ uint32_t inv(uint32_t v)
@@ -193,12 +205,18 @@ __device__ __forceinline__ uint32_t inv(uint32_t v)
 
 __device__ __forceinline__ uint64_t inv(uint64_t v)
 {
-  v = (v >> 1) ^ static_cast<uint64_t>(static_cast<int64_t>(v << 63) >> 63);
-  if (v & 0xffe0000000000000ull) {
-    if (v >= 0x8000000000000000ull) v += 0x0020000000000000ull;
-    v += 0x8000000000000000ull;
+  const uint32_t h = static_cast<uint32_t>(v >> 32);
+  const uint32_t l = static_cast<uint32_t>(v);
+  const uint32_t sg = 0u - (l & 1u);                       // (v << 63) >> 63 arithmetic
+  uint32_t nh = (h >> 1) ^ sg;
+  const uint32_t nl = __funnelshift_r(l, h, 1) ^ sg;
+  if (nh & 0xffe00000u) {
+    if (nh >= 0x80000000u) nh += 0x00200000u;
+    nh += 0x80000000u;
   }
-  return (v << 63) | (v >> 1);
+  const uint32_t oh = __funnelshift_r(nh, nl, 1);          // rotate right by 1
+  const uint32_t ol = __funnelshift_r(nl, nh, 1);
+  return (static_cast<uint64_t>(oh) << 32) | ol;
 }
 
 __device__ __forceinline__ uint32_t quant(uint32_t val, const QParams& q)
@@ -382,46 +400,79 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
 // ----------------------------------------------------------------------------
 // Shifted store: writes `len` bytes from 16-byte aligned shared memory `src`
 // to the arbitrary global byte address `dst`.  Whole aligned 16-byte granules
-// use one vector store; the (at most two) granules shared with neighbouring
-// chunks are written byte by byte.  Called by all NT threads.
+// get one vector store each (a thread handles two neighbouring granules from
+// three aligned shared loads); the at most two granules shared with
+// neighbouring chunks are written byte by byte.  Called by all NT threads.
 // ----------------------------------------------------------------------------
+template <int WQ>
+__device__ __forceinline__ void shifted_pair(uint4* out, const uint4* s4, int j, int nfull_end, int bb8)
+{
+  // output granules j and j+1 from source blocks j-1, j, j+1 (j >= 1)
+  const uint4 x = s4[j - 1];
+  const uint4 y = s4[j];
+  const uint32_t w[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+  uint4 o;
+  o.x = __funnelshift_r(w[WQ + 0], w[WQ + 1], bb8);
+  o.y = __funnelshift_r(w[WQ + 1], w[WQ + 2], bb8);
+  o.z = __funnelshift_r(w[WQ + 2], w[WQ + 3], bb8);
+  o.w = __funnelshift_r(w[WQ + 3], w[WQ + 4], bb8);
+  out[j] = o;
+  if (j + 1 < nfull_end) {
+    const uint4 z = s4[j + 1];
+    const uint32_t u[8] = {y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w};
+    o.x = __funnelshift_r(u[WQ + 0], u[WQ + 1], bb8);
+    o.y = __funnelshift_r(u[WQ + 1], u[WQ + 2], bb8);
+    o.z = __funnelshift_r(u[WQ + 2], u[WQ + 3], bb8);
+    o.w = __funnelshift_r(u[WQ + 3], u[WQ + 4], bb8);
+    out[j + 1] = o;
+  }
+}
+
 template <int NT>
 __device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len)
 {
+  const int tid = threadIdx.x;
   const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
   const int sft = static_cast<int>(d & 15u);
   uint8_t* const a0 = dst - sft;
-  const int nunits = (sft + len + 15) >> 4;
+  uint4* const out = reinterpret_cast<uint4*>(a0);
   const uint4* const s4 = reinterpret_cast<const uint4*>(src);
-  const int bo = (16 - sft) & 15;
-  const int wq = bo >> 2;
-  const int bb8 = (bo & 3) * 8;
-  for (int j = threadIdx.x; j < nunits; j += NT) {
-    const int r = 16 * j - sft;
-    if (r >= 0 && r + 16 <= len) {
-      uint4 o;
-      if (sft == 0) {
-        o = s4[j];
-      } else {
-        const uint4 x = s4[j - 1];
-        const uint4 y = s4[j];
-        uint32_t a[5];
-        switch (wq) {
-          case 0: a[0] = x.x; a[1] = x.y; a[2] = x.z; a[3] = x.w; a[4] = y.x; break;
-          case 1: a[0] = x.y; a[1] = x.z; a[2] = x.w; a[3] = y.x; a[4] = y.y; break;
-          case 2: a[0] = x.z; a[1] = x.w; a[2] = y.x; a[3] = y.y; a[4] = y.z; break;
-          default: a[0] = x.w; a[1] = y.x; a[2] = y.y; a[3] = y.z; a[4] = y.w; break;
-        }
-        o.x = __funnelshift_r(a[0], a[1], bb8);
-        o.y = __funnelshift_r(a[1], a[2], bb8);
-        o.z = __funnelshift_r(a[2], a[3], bb8);
-        o.w = __funnelshift_r(a[3], a[4], bb8);
-      }
-      *reinterpret_cast<uint4*>(a0 + 16 * j) = o;
-    } else {
+  const int nunits = (sft + len + 15) >> 4;
+  const int jf = sft ? 1 : 0;              // first granule entirely inside the chunk
+  const int jl = (sft + len) >> 4;         // one past the last such granule
+  if (sft == 0) {
+    for (int j = tid; j < jl; j += NT) out[j] = s4[j];
+  } else {
+    const int bo = 16 - sft;
+    const int bb8 = (bo & 3) * 8;
+    switch (bo >> 2) {
+      case 0:
+        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<0>(out, s4, j, jl, bb8);
+        break;
+      case 1:
+        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<1>(out, s4, j, jl, bb8);
+        break;
+      case 2:
+        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<2>(out, s4, j, jl, bb8);
+        break;
+      default:
+        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<3>(out, s4, j, jl, bb8);
+        break;
+    }
+  }
+  // edge granules (shared with the neighbouring chunks): byte stores
+  if (tid < 2) {
+    int e = -1;
+    if (tid == 0 && sft != 0) e = 0;
+    if (tid == 1) {
+      const int last = nunits - 1;
+      if (last >= jl && !(last == 0 && sft != 0)) e = last;
+    }
+    if (e >= 0) {
+      const int r = 16 * e - sft;
       const int b0 = r < 0 ? -r : 0;
       const int b1 = (len - r) < 16 ? (len - r) : 16;
-      for (int b = b0; b < b1; b++) a0[16 * j + b] = src[r + b];
+      for (int b = b0; b < b1; b++) a0[16 * e + b] = src[r + b];
     }
   }
 }

@@ -68,20 +68,25 @@ __device__ __forceinline__ bool cbar_or(bool pred)
   return r != 0;
 }
 
-// Appends the bits of the stream in order and hands out each completed 32-bit
-// word: the first one is kept (its low bits belong to the previous lane), the
-// others are stored at consecutive word slots.
-struct WordSink {
-  uint32_t* dst;  // slot of the lane's first word
-  uint32_t first;
-  int j;
-  __device__ __forceinline__ void emit(uint32_t w)
-  {
-    if (j == 0) first = w;
-    else dst[j] = w;
-    ++j;
+// ORs `v`, placed at bit offset `o` (< 96, warp-uniform) of a 128-bit run, into
+// the run's words x0..x3.
+__device__ __forceinline__ void place32(uint32_t v, int o, uint32_t& x0, uint32_t& x1, uint32_t& x2, uint32_t& x3)
+{
+  const int q = o >> 5;
+  const int r = o & 31;
+  const uint32_t lo = v << r;
+  const uint32_t hi = __funnelshift_l(v, 0u, r);  // bits that cross into the next word
+  if (q == 0) {
+    x0 |= lo;
+    x1 |= hi;
+  } else if (q == 1) {
+    x1 |= lo;
+    x2 |= hi;
+  } else {
+    x2 |= lo;
+    x3 |= hi;
   }
-};
+}
 
 // Packs one subchunk whose transformed values sit in registers: lane L holds
 // values P*L .. P*L+P-1 and writes the bit run [P*L*ln, P*(L+1)*ln) of the
@@ -111,39 +116,42 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
   const int w0 = rs >> 5;
   const int s = rs & 31;
   if (R >= 32) {
-    // each word holds bits of at most two adjacent lanes: exchange one partial word
-    WordSink out{pw + w0, 0u, 0};
-    uint64_t acc = 0;
-    int n = s;
-#pragma unroll
-    for (int k = 0; k < P; ++k) {
-      if constexpr (sizeof(T) == 4) {
-        acc |= static_cast<uint64_t>(v[k]) << n;
-        n += ln;
-        if (n >= 32) {
-          out.emit(static_cast<uint32_t>(acc));
-          acc >>= 32;
-          n -= 32;
-        }
-      } else {
-        uint64_t lo = acc | (v[k] << n);
-        const uint32_t hi = n ? static_cast<uint32_t>(v[k] >> (64 - n)) : 0u;
-        n += ln;
-        if (n >= 32) {
-          out.emit(static_cast<uint32_t>(lo));
-          lo = (lo >> 32) | (static_cast<uint64_t>(hi) << 32);
-          n -= 32;
-          if (n >= 32) {
-            out.emit(static_cast<uint32_t>(lo));
-            lo >>= 32;
-            n -= 32;
-          }
-        }
-        acc = lo;
+    // the run as a 128-bit number x3:x2:x1:x0 (the offsets are warp-uniform)
+    uint32_t x0, x1 = 0u, x2 = 0u, x3 = 0u;
+    if constexpr (sizeof(T) == 4) {
+      x0 = v[0];
+      place32(v[1], ln, x0, x1, x2, x3);
+      place32(v[2], 2 * ln, x0, x1, x2, x3);
+      place32(v[3], 3 * ln, x0, x1, x2, x3);
+    } else {
+      const uint32_t a0 = static_cast<uint32_t>(v[0]), a1 = static_cast<uint32_t>(v[0] >> 32);
+      const uint32_t b0 = static_cast<uint32_t>(v[1]), b1 = static_cast<uint32_t>(v[1] >> 32);
+      if (ln >= 32) {
+        const int r = ln - 32;
+        x0 = a0;
+        x1 = a1 | (b0 << r);
+        x2 = __funnelshift_l(b0, b1, r);
+        x3 = __funnelshift_l(b1, 0u, r);
+      } else {  // both values fit in 31 bits
+        x0 = a0 | (b0 << ln);
+        x1 = __funnelshift_l(b0, 0u, ln);
       }
     }
-    const uint32_t prev = __shfl_up_sync(0xffffffffu, static_cast<uint32_t>(acc), 1);
-    pw[w0] = s ? (out.first | prev) : out.first;
+    // shifted into place within the lane's first word
+    const uint32_t y0 = x0 << s;
+    const uint32_t y1 = __funnelshift_l(x0, x1, s);
+    const uint32_t y2 = __funnelshift_l(x1, x2, s);
+    const uint32_t y3 = __funnelshift_l(x2, x3, s);
+    const uint32_t y4 = __funnelshift_l(x3, 0u, s);
+    const int nfull = (s + R) >> 5;  // words 1 .. nfull-1 lie wholly in this run
+    const uint32_t tail = nfull == 1 ? y1 : (nfull == 2 ? y2 : (nfull == 3 ? y3 : y4));
+    // each word holds bits of at most two adjacent lanes: the next lane completes our tail
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, tail, 1);
+    uint32_t* const d = pw + w0;
+    d[0] = s ? (y0 | prev) : y0;
+    if (nfull > 1) d[1] = y1;
+    if (nfull > 2) d[2] = y2;
+    if (nfull > 3) d[3] = y3;
   } else {
     // short runs: several lanes share a word; clear the words, then OR in
     const int words = (32 * P * ln) >> 5;
