@@ -44,6 +44,7 @@ extern "C" {
 #define SLEEK_ERR_WORKSPACE      7  /* caller workspace smaller than required */
 #define SLEEK_ERR_NO_DEVICE      8  /* no CUDA device */
 #define SLEEK_ERR_CAPACITY       9  /* output buffer smaller than required */
+#define SLEEK_ERR_TOO_LARGE     10  /* input larger than SLEEK_STATIC_MAX_INPUT_BYTES (static-scratch entry point) */
 
 /* Human-readable name of a status code. */
 const char* sleek_status_string(int status);
@@ -111,6 +112,22 @@ int sleek_decompress_lossy_f32(sleek_eb_info_f32 eb, const unsigned char* d_enco
 int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* d_encoded, long long encoded_bytes,
                                double* d_decoded, long long decoded_capacity, long long* d_decsize,
                                void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Lossless float32 compress that allocates no device memory, for callers that cannot
+ * call cudaMalloc (device memory owned by a framework or pool allocator, a fixed memory
+ * budget, or a path that must not risk the device synchronisation an allocation can
+ * cause).  This entry point has no counterpart in the reference.  Its scratch is a
+ * file-scope device array inside the library (512 KiB per device, held until the process
+ * exits), so inputs are limited to SLEEK_STATIC_MAX_INPUT_BYTES (1 GiB); larger ones are
+ * rejected with SLEEK_ERR_TOO_LARGE.  The first call on a device looks up the scratch's
+ * device address (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the one scratch and it keeps the last call's
+ * contents (each call clears what it needs on `stream`), so calls whose executions overlap
+ * on the GPU (different streams, no ordering between them) race: order them on one stream.
+ * Output, stream format and errors are those of sleek_compress_f32. */
+#define SLEEK_STATIC_MAX_INPUT_BYTES (1ll << 30)
+int sleek_compress_f32_static(const float* d_input, long long num_elements, unsigned char* d_encoded,
+                              long long* d_encsize, void* stream);
 
 /* Synchronises `stream` and reads the device status of the last call that used
  * d_workspace (NULL = the library-owned workspace of the current device and

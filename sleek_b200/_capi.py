@@ -24,6 +24,7 @@ SLEEK_ERR_TIMEOUT = 6
 SLEEK_ERR_WORKSPACE = 7
 SLEEK_ERR_NO_DEVICE = 8
 SLEEK_ERR_CAPACITY = 9
+SLEEK_ERR_TOO_LARGE = 10
 
 
 class EbInfoF32(C.Structure):
@@ -56,6 +57,7 @@ SIGNATURES = {
     "sleek_decompress_lossy_f32": (C.c_int, [EbInfoF32, _vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
     "sleek_decompress_lossy_f64": (C.c_int, [EbInfoF64, _vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+    "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -199,6 +199,7 @@ const char* sleek_status_string(int s)
     case SLEEK_ERR_WORKSPACE: return "workspace too small";
     case SLEEK_ERR_NO_DEVICE: return "no CUDA device";
     case SLEEK_ERR_CAPACITY: return "output capacity exceeded";
+    case SLEEK_ERR_TOO_LARGE: return "input larger than the static scratch allows";
     default: return "unknown status";
   }
 }
