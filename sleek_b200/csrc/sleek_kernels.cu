@@ -202,49 +202,63 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
     // look-back wait for it.
-    if (lane == 0) {
-      unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
-      unsigned issued = 0;      // stages whose last use was a TMA copy
-      unsigned issued_par = 0;  // parity of that use
-      bool more = true;
-      for (int seq = 0;; ++seq) {
-        const int s = seq % ENC_STAGES;
-        // From seq 2 on, the copy for chunk seq is issued when the compute warps
-        // start chunk seq - 1: one chunk of lookahead, and the stage's previous
-        // chunk (seq - 4) has been stored by then.
-        if (seq >= 2) {
-          if (!mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1)) {
-            set_status(ws, ST_TIMEOUT, -1);
-            break;
-          }
+    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
+    unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
+    unsigned issued_par = 0;  // parity of that use
+    bool more = true;
+    for (int seq = 0;; ++seq) {
+      const int s = seq % ENC_STAGES;
+      // From seq 2 on, the copy for chunk seq is issued when the compute warps
+      // start chunk seq - 1: one chunk of lookahead, and the stage's previous
+      // chunk (seq - 4) has been stored by then.
+      if (seq >= 2) {
+        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+          if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
+          break;
         }
-        const long long t = more ? static_cast<long long>(atomicAdd(tick, 1ull)) : NO_CHUNK;
-        EncMeta& me = m.meta[s];
-        bool copy = false;
-        if (t < chunks) {
-          const long long base = t * CS;
-          const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-          const uint32_t tbytes = in_aligned ? static_cast<uint32_t>(osize & ~15) : 0u;
-          me.c = t;
-          if (tbytes) {
-            mbar_arrive_expect_tx(&m.full[s], tbytes);
-            tma_load_1d(stage0 + s * STAGE_BYTES, a.in + base, tbytes, &m.full[s]);
-            copy = true;
+      }
+      long long t = NO_CHUNK;
+      if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
+      t = __shfl_sync(0xffffffffu, t, 0);
+      uint8_t* const stg = stage0 + s * STAGE_BYTES;
+      if (t < chunks) {
+        const long long base = t * CS;
+        const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
+        if (in_aligned && osize == CS) {
+          if (lane == 0) {
+            m.meta[s].c = t;
+            mbar_arrive_expect_tx(&m.full[s], CS);
+            tma_load_1d(stg, a.in + base, CS, &m.full[s]);
+            issued |= 1u << s;
+            issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
           }
         } else {
-          me.c = NO_CHUNK;
-          more = false;
+          // last partial chunk or an input that is not 16-byte aligned: element
+          // loads, zero padding up to the full chunk (the padding is encoded too)
+          const int elem = static_cast<int>(sizeof(T));
+          const T* const gin = reinterpret_cast<const T*>(a.in + base);
+          T* const sv = reinterpret_cast<T*>(stg);
+          for (int k = lane; k < CS / elem; k += 32) sv[k] = k * elem < osize ? gin[k] : T(0);
+          __syncwarp();
+          if (lane == 0) {
+            m.meta[s].c = t;
+            issued &= ~(1u << s);
+            mbar_arrive(&m.full[s]);  // release: the stores above are visible to its waiters
+          }
         }
-        if (copy) {
-          issued |= 1u << s;
-          issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
-        } else {
+      } else {
+        more = false;
+        if (lane == 0) {
+          m.meta[s].c = NO_CHUNK;
           issued &= ~(1u << s);
           mbar_arrive(&m.full[s]);
         }
-        if (!more) break;
       }
-      // never leave with a bulk copy still landing in this CTA's shared memory
+      if (!more) break;
+    }
+    // never leave with a bulk copy still landing in this CTA's shared memory
+    if (lane == 0) {
       for (int s = 0; s < ENC_STAGES; ++s)
         if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
@@ -314,38 +328,19 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
 
       // ---- phase A: values into registers, transform / quantize, bit widths ----
+      // (the stage always holds a full 16 KB chunk: partial chunks are zero padded)
       const long long base = c * CS;
       const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-      const int tbytes = in_aligned ? (osize & ~15) : 0;
       T vals[SPW][P];
 #pragma unroll
       for (int u = 0; u < SPW; ++u) {
         const int i = cw + u * ENC_CW;
-        const int k0 = i * V::VPS + lane * P;  // first value of this lane in the chunk
-        if (tbytes == CS) {
-          const uint4 q = *reinterpret_cast<const uint4*>(stg + k0 * sizeof(T));
-          if constexpr (sizeof(T) == 4) {
-            vals[u][0] = q.x; vals[u][1] = q.y; vals[u][2] = q.z; vals[u][3] = q.w;
-          } else {
-            vals[u][0] = (static_cast<uint64_t>(q.y) << 32) | q.x;
-            vals[u][1] = (static_cast<uint64_t>(q.w) << 32) | q.z;
-          }
+        const uint4 q = *reinterpret_cast<const uint4*>(stg + i * 512 + lane * 16);
+        if constexpr (sizeof(T) == 4) {
+          vals[u][0] = q.x; vals[u][1] = q.y; vals[u][2] = q.z; vals[u][3] = q.w;
         } else {
-          T* const sv = reinterpret_cast<T*>(stg);
-          const T* const gin = reinterpret_cast<const T*>(a.in + base);
-#pragma unroll
-          for (int p = 0; p < P; ++p) {
-            const int k = k0 + p;
-            const int b = k * static_cast<int>(sizeof(T));
-            T x = 0;
-            if (b < tbytes) {
-              x = sv[k];
-            } else if (b < osize) {
-              x = gin[k];
-              sv[k] = x;  // keep the staged copy complete for a raw store
-            }
-            vals[u][p] = x;  // zero padding is transformed too
-          }
+          vals[u][0] = (static_cast<uint64_t>(q.y) << 32) | q.x;
+          vals[u][1] = (static_cast<uint64_t>(q.w) << 32) | q.z;
         }
         T orv = 0;
 #pragma unroll
