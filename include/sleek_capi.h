@@ -129,6 +129,41 @@ int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* d_enco
 int sleek_compress_f32_static(const float* d_input, long long num_elements, unsigned char* d_encoded,
                               long long* d_encsize, void* stream);
 
+/* ---- batched compress / decompress ---------------------------------------------
+ * Many buffers of uneven sizes with mixed float32 / float64 and mixed error bounds in
+ * one persistent launch (per group of up to 1024 buffers).  The batched form has no
+ * single counterpart in the reference, whose API takes one buffer per call
+ * (include/sleek_lossless_gpu.h:47-100, include/sleek_lossy_gpu.h:74-127); every buffer's
+ * stream is bit-identical to what the single-buffer call produces for it. */
+typedef struct {
+  const void* input;        /* compress: device values; decompress: device stream (8-byte aligned) */
+  void* output;             /* compress: device stream, >= sleek_upper_bound_size bytes; decompress: device values */
+  long long* size_out;      /* device: bytes written (stream or decoded), or -status */
+  long long num_elements;   /* compress: input elements; decompress: output capacity in elements */
+  long long stream_bytes;   /* decompress: stream length, -1 = trust the stream; ignored by compress */
+  int elem_bytes;           /* 4 = float, 8 = double */
+  int lossy;                /* 0 = lossless, 1 = absolute error bound */
+  double error_bound;       /* lossy only; same rules as sleek_error_bound_f32/_f64 */
+} sleek_batch_item;
+
+typedef struct sleek_batch_plan sleek_batch_plan;
+
+/* Validates the items, derives the quantizer parameters and uploads the job tables
+ * (allocates device memory and synchronises: call it outside stream capture). */
+int sleek_batch_plan_create(const sleek_batch_item* items, int n, int decompress, sleek_batch_plan** plan);
+/* Workspace bytes a run of the plan needs. */
+size_t sleek_batch_plan_workspace_size(const sleek_batch_plan* plan);
+/* Tuning: CTAs per SM of the plan's launches (0 = as many as fit). */
+int sleek_batch_plan_set_grid(sleek_batch_plan* plan, int ctas_per_sm);
+/* Clears the workspace and launches on `stream`: no host work and no allocation, so a
+ * run can be captured in a CUDA graph.  Runs sharing a workspace must be stream-ordered. */
+int sleek_batch_plan_run(sleek_batch_plan* plan, void* d_workspace, size_t workspace_bytes, void* stream);
+int sleek_batch_plan_destroy(sleek_batch_plan* plan);
+/* One-shot forms: create a plan, run it, wait for `stream`, destroy it (d_workspace
+ * may be NULL: then a temporary one is allocated). */
+int sleek_compress_batch(const sleek_batch_item* items, int n, void* d_workspace, size_t workspace_bytes, void* stream);
+int sleek_decompress_batch(const sleek_batch_item* items, int n, void* d_workspace, size_t workspace_bytes, void* stream);
+
 /* Synchronises `stream` and reads the device status of the last call that used
  * d_workspace (NULL = the library-owned workspace of the current device and
  * `stream`).  *status receives SLEEK_OK or the first device-side error. */

@@ -35,6 +35,12 @@ class EbInfoF64(C.Structure):
     _fields_ = [("eb_e", C.c_int), ("thr_e", C.c_int), ("offs_e", C.c_ulonglong)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("input", C.c_void_p), ("output", C.c_void_p), ("size_out", C.c_void_p),
+                ("num_elements", C.c_longlong), ("stream_bytes", C.c_longlong),
+                ("elem_bytes", C.c_int), ("lossy", C.c_int), ("error_bound", C.c_double)]
+
+
 # every symbol the header declares: name -> (restype, argtypes)
 _i64 = C.c_longlong
 _vp = C.c_void_p
@@ -58,6 +64,13 @@ SIGNATURES = {
     "sleek_decompress_lossy_f64": (C.c_int, [EbInfoF64, _vp, _i64, _vp, _i64, _vp, _vp, _sz, _vp]),
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
+    "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "sleek_batch_plan_workspace_size": (_sz, [_vp]),
+    "sleek_batch_plan_set_grid": (C.c_int, [_vp, C.c_int]),
+    "sleek_batch_plan_run": (C.c_int, [_vp, _vp, _sz, _vp]),
+    "sleek_batch_plan_destroy": (C.c_int, [_vp]),
+    "sleek_compress_batch": (C.c_int, [C.c_void_p, C.c_int, _vp, _sz, _vp]),
+    "sleek_decompress_batch": (C.c_int, [C.c_void_p, C.c_int, _vp, _sz, _vp]),
 }
 
 _lib = None

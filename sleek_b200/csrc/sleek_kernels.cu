@@ -28,13 +28,21 @@ constexpr int ENC_NT = (ENC_CW + 2) * 32;    // + a producer warp and a scanner 
 constexpr int ENC_MINB = 3;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
+// What the producer tells the compute and scanner warps about the chunk in a stage.
 struct EncMeta {
-  long long c;     // chunk id, or NO_CHUNK: no more work for this CTA
-  long long excl;  // byte offset of the chunk's payload (or -1 after an error)
+  long long g;          // look-back flag index (chunk id across the launch), or NO_CHUNK
+  long long c;          // chunk index within its buffer
+  long long seg;        // flag index of the buffer's first chunk
+  long long chunks;     // chunks of the buffer
+  long long insize;     // bytes of the buffer
+  uint8_t* out;         // the buffer's stream
+  long long* outsize;   // the buffer's size output
+  long long excl;       // payload offset of the chunk (scanner), -1 after an error
+  QParams q;            // the buffer's quantizer parameters
+  int kind;             // bit 0: 64-bit values, bit 1: lossy
   int osize;
   int csize;
   int comp;
-  int pad_;
 };
 
 struct EncMisc {
@@ -47,6 +55,7 @@ struct EncMisc {
 };
 
 constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
+constexpr int ENC_BATCH_SMEM = ENC_SMEM + 8 * (BATCH_MAX_JOBS + 1);  // + the jobs' first chunk ids
 
 // barrier among the compute warps only (named barrier 1)
 __device__ __forceinline__ void cbar()
@@ -166,26 +175,155 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
   }
 }
 
-template <typename T, bool LOSSY, int MINB>
-__global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
+
+// Transform, size, publish and pack one chunk (compute warps).  KIND: bit 0 =
+// 64-bit values, bit 1 = lossy.
+template <int KIND>
+__device__ __forceinline__ void compute_chunk(uint8_t* stg, EncMeta& me, EncMisc& m, uint64_t* flags, int cw,
+                                              int lane, int tid)
 {
+  using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
+  constexpr bool LOSSY = (KIND & 2) != 0;
   using V = VT<T>;
   constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane per subchunk
   constexpr int SPW = SC / ENC_CW;                      // subchunks per compute warp
+  const QParams q = me.q;
+  const int osize = me.osize;
+
+  // ---- phase A: values into registers, transform / quantize, bit widths ------
+  // (the stage always holds a full 16 KB chunk: partial chunks are zero padded)
+  T vals[SPW][P];
+#pragma unroll
+  for (int u = 0; u < SPW; ++u) {
+    const int i = cw + u * ENC_CW;
+    const uint4 w4 = *reinterpret_cast<const uint4*>(stg + i * 512 + lane * 16);
+    if constexpr (sizeof(T) == 4) {
+      vals[u][0] = w4.x; vals[u][1] = w4.y; vals[u][2] = w4.z; vals[u][3] = w4.w;
+    } else {
+      vals[u][0] = (static_cast<uint64_t>(w4.y) << 32) | w4.x;
+      vals[u][1] = (static_cast<uint64_t>(w4.w) << 32) | w4.z;
+    }
+    T orv = 0;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      vals[u][p] = encode_value<LOSSY>(vals[u][p], q);
+      orv |= vals[u][p];
+    }
+    const int w = warp_bit_width(orv);
+    if (lane == 0) m.lnv[i] = w;
+  }
+  cbar();
+
+  // ---- widths scan (every warp, redundantly), size decision -----------------
+  const int ln_l = m.lnv[lane];
+  const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
+  int incl = wc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+  const int newsize = 34 + 4 * wtot;
+  const bool comp = newsize < osize;
+  const int csize = comp ? newsize : osize;
+  if (tid == 0) {
+    me.csize = csize;
+    me.comp = comp;
+    st_relaxed_u64(&flags[me.g], (me.c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+    mbar_arrive(&m.sized[&me - m.meta]);
+  }
+
+  // ---- pack this chunk from registers ----------------------------------------
+  if (comp) {
+    uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
+#pragma unroll
+    for (int u = 0; u < SPW; ++u) {
+      const int i = cw + u * ENC_CW;
+      const int wbase = __shfl_sync(0xffffffffu, incl - wc, i);
+      const int ln = __shfl_sync(0xffffffffu, ln_l, i);
+      pack_subchunk<T>(pw + wbase, ln, vals[u], lane);
+    }
+    if (cw == 0) {
+      stg[lane] = static_cast<uint8_t>(ln_l);
+      if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
+    }
+  }
+}
+
+// Chunk sources: one buffer (the plain entry points) or a table of buffers (the
+// batched entry points; every chunk of every buffer is one ticket).
+template <bool BATCH>
+struct EncSource;
+
+template <>
+struct EncSource<false> {
+  const EncArgs& a;
+  long long chunks;
+  __device__ long long total() const { return chunks; }
+  // fills the chunk's description; returns its first byte
+  __device__ const uint8_t* describe(long long g, EncMeta& me, int kind) const
+  {
+    me.g = g;
+    me.c = g;
+    me.seg = 0;
+    me.chunks = chunks;
+    me.insize = a.insize;
+    me.out = a.out;
+    me.outsize = a.outsize;
+    me.q = a.q;
+    me.kind = kind;
+    me.osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - g * CS));
+    return a.in + g * CS;
+  }
+};
+
+template <>
+struct EncSource<true> {
+  const BatchEncArgs& a;
+  const long long* cb;  // shared memory: first chunk id of each job, then the total
+  __device__ long long total() const { return cb[a.njobs]; }
+  __device__ const uint8_t* describe(long long g, EncMeta& me, int) const
+  {
+    int lo = 0, hi = a.njobs - 1;  // last job whose first chunk id is <= g (empty jobs are skipped)
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cb[mid] <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchJob& j = a.jobs[lo];
+    const long long c = g - cb[lo];
+    me.g = g;
+    me.c = c;
+    me.seg = cb[lo];
+    me.chunks = j.chunks;
+    me.insize = j.insize;
+    me.out = j.out;
+    me.outsize = j.outsize;
+    me.q = j.q;
+    me.kind = j.kind;
+    me.osize = static_cast<int>(min(static_cast<long long>(CS), j.insize - c * CS));
+    return j.in + c * CS;
+  }
+};
+
+template <int KIND, bool BATCH, int MINB>
+__global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::conditional<BATCH, BatchEncArgs, EncArgs>::type a)
+{
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const stage0 = smem;
   EncMisc& m = *reinterpret_cast<EncMisc*>(smem + ENC_STAGES * STAGE_BYTES);
+  long long* const cb = reinterpret_cast<long long*>(smem + ENC_SMEM);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const long long chunks = (a.insize + CS - 1) / CS;
   uint64_t* const ws = a.ws;
   uint64_t* const flags = ws + WS_HDR_WORDS;
-  uint8_t* const size_out = a.out + 8;
-  uint8_t* const data_out = a.out + 8 + 2 * chunks;
-  const bool in_aligned = (reinterpret_cast<uintptr_t>(a.in) & 15u) == 0u;
 
+  if constexpr (BATCH) {
+    for (int i = tid; i <= a.njobs; i += ENC_NT) cb[i] = a.chunk_base[i];
+  }
   if (tid == 0) {
     for (int s = 0; s < ENC_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
@@ -196,6 +334,12 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
     mbar_fence_init();
   }
   __syncthreads();
+
+  EncSource<BATCH> src = [&]() {
+    if constexpr (BATCH) return EncSource<true>{a, cb};
+    else return EncSource<false>{a, (a.insize + CS - 1) / CS};
+  }();
+  const long long total = src.total();
 
   if (warp == ENC_CW) {
     // ===================== producer warp: tickets and TMA copies =====================
@@ -222,27 +366,29 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
       if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
       t = __shfl_sync(0xffffffffu, t, 0);
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
-      if (t < chunks) {
-        const long long base = t * CS;
-        const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-        if (in_aligned && osize == CS) {
+      EncMeta& me = m.meta[s];
+      if (t < total) {
+        const uint8_t* in = nullptr;
+        if (lane == 0) in = src.describe(t, me, KIND);
+        __syncwarp();
+        in = reinterpret_cast<const uint8_t*>(__shfl_sync(0xffffffffu, reinterpret_cast<uintptr_t>(in), 0));
+        const int osize = me.osize;
+        if ((reinterpret_cast<uintptr_t>(in) & 15u) == 0u && osize == CS) {
           if (lane == 0) {
-            m.meta[s].c = t;
             mbar_arrive_expect_tx(&m.full[s], CS);
-            tma_load_1d(stg, a.in + base, CS, &m.full[s]);
+            tma_load_1d(stg, in, CS, &m.full[s]);
             issued |= 1u << s;
             issued_par = (issued_par & ~(1u << s)) | (((seq / ENC_STAGES) & 1u) << s);
           }
         } else {
-          // last partial chunk or an input that is not 16-byte aligned: element
-          // loads, zero padding up to the full chunk (the padding is encoded too)
-          const int elem = static_cast<int>(sizeof(T));
-          const T* const gin = reinterpret_cast<const T*>(a.in + base);
-          T* const sv = reinterpret_cast<T*>(stg);
-          for (int k = lane; k < CS / elem; k += 32) sv[k] = k * elem < osize ? gin[k] : T(0);
+          // last partial chunk or an input that is not 16-byte aligned: 4-byte
+          // loads (inputs are at least 4-byte aligned), zero padding up to the full
+          // chunk (the padding is encoded too)
+          const uint32_t* const gin = reinterpret_cast<const uint32_t*>(in);
+          uint32_t* const sv = reinterpret_cast<uint32_t*>(stg);
+          for (int k = lane; k < CS / 4; k += 32) sv[k] = 4 * k < osize ? gin[k] : 0u;
           __syncwarp();
           if (lane == 0) {
-            m.meta[s].c = t;
             issued &= ~(1u << s);
             mbar_arrive(&m.full[s]);  // release: the stores above are visible to its waiters
           }
@@ -250,7 +396,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
       } else {
         more = false;
         if (lane == 0) {
-          m.meta[s].c = NO_CHUNK;
+          me.g = NO_CHUNK;
           issued &= ~(1u << s);
           mbar_arrive(&m.full[s]);
         }
@@ -269,31 +415,40 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
       const uint32_t par = (seq / ENC_STAGES) & 1;
       bool ok = mbar_wait_bounded(&m.full[s], par);
       if (__any_sync(0xffffffffu, !ok)) break;  // the compute warps report it
-      const long long c = m.meta[s].c;
-      if (c == NO_CHUNK) break;
+      EncMeta& me = m.meta[s];
+      const long long g = me.g;
+      if (g == NO_CHUNK) break;
       ok = mbar_wait_bounded(&m.sized[s], par);
       if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, c);
+        if (lane == 0) set_status(ws, ST_TIMEOUT, g);
         break;
       }
-      const int csize = m.meta[s].csize;
+      const long long c = me.c;
+      const int csize = me.csize;
       long long excl = 0;
       if (c > 0) {
-        excl = lookback(flags, c, 0, ws);
+        excl = lookback(flags, g, me.seg, ws);
         unsigned err = 0;
         if (excl < 0) err = ST_TIMEOUT;
         else if (excl > c * CS) err = ST_CAPACITY;
         if (err) excl = -1;
         if (lane == 0) {
-          if (err) set_status(ws, err, c);
+          if (err) set_status(ws, err, g);
           // an impossible prefix is replaced by the largest legal one so that
           // every later chunk still writes inside the output bound
-          st_relaxed_u64(&flags[c], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
+          st_relaxed_u64(&flags[g], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
         }
       }
       if (lane == 0) {
-        m.meta[s].excl = excl;
-        if (c == chunks - 1 && excl >= 0) ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
+        me.excl = excl;
+        if (c == me.chunks - 1 && excl >= 0) {
+          if constexpr (BATCH) {  // the buffer is complete: its header and size
+            *reinterpret_cast<long long*>(me.out) = me.insize;
+            *me.outsize = 8 + 2 * me.chunks + excl + csize;
+          } else {
+            ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
+          }
+        }
         mbar_arrive(&m.placed[s]);
       }
     }
@@ -302,10 +457,14 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
     const int cw = warp;
     auto store = [&](int sq) {  // all compute threads; placed[] already observed
       const int sp = sq % ENC_STAGES;
-      const EncMeta me = m.meta[sp];
-      if (me.excl >= 0) {
-        store_shifted<ENC_CW * 32>(data_out + me.excl, stage0 + sp * STAGE_BYTES, me.csize);
-        if (tid == 0) *reinterpret_cast<uint16_t*>(size_out + 2 * me.c) = static_cast<uint16_t>(me.csize);
+      const EncMeta& me = m.meta[sp];
+      const long long excl = me.excl;
+      if (excl >= 0) {
+        uint8_t* const out = me.out;
+        const long long c = me.c;
+        const int csize = me.csize;
+        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize);
+        if (tid == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
       }
     };
 
@@ -323,73 +482,19 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
       // start of chunk seq: the producer may copy chunk seq + 1 into the stage of
       // seq - 3, whose store every compute warp has finished
       if (seq >= 1 && tid == 0) mbar_arrive(&m.empty[(seq + 1) % ENC_STAGES]);
-      const long long c = m.meta[s].c;
-      if (c == NO_CHUNK) break;
+      EncMeta& me = m.meta[s];
+      if (me.g == NO_CHUNK) break;
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
-
-      // ---- phase A: values into registers, transform / quantize, bit widths ----
-      // (the stage always holds a full 16 KB chunk: partial chunks are zero padded)
-      const long long base = c * CS;
-      const int osize = static_cast<int>(min(static_cast<long long>(CS), a.insize - base));
-      T vals[SPW][P];
-#pragma unroll
-      for (int u = 0; u < SPW; ++u) {
-        const int i = cw + u * ENC_CW;
-        const uint4 q = *reinterpret_cast<const uint4*>(stg + i * 512 + lane * 16);
-        if constexpr (sizeof(T) == 4) {
-          vals[u][0] = q.x; vals[u][1] = q.y; vals[u][2] = q.z; vals[u][3] = q.w;
-        } else {
-          vals[u][0] = (static_cast<uint64_t>(q.y) << 32) | q.x;
-          vals[u][1] = (static_cast<uint64_t>(q.w) << 32) | q.z;
-        }
-        T orv = 0;
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          vals[u][p] = encode_value<LOSSY>(vals[u][p], a.q);
-          orv |= vals[u][p];
-        }
-        const int w = warp_bit_width(orv);
-        if (lane == 0) m.lnv[i] = w;
-      }
-      cbar();
-
-      // ---- widths scan (every warp, redundantly), size decision ---------------
-      const int ln_l = m.lnv[lane];
-      const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
-      int incl = wc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-      }
-      const int wtot = __shfl_sync(0xffffffffu, incl, 31);
-      const int newsize = 34 + 4 * wtot;
-      const bool comp = newsize < osize;
-      const int csize = comp ? newsize : osize;
-      if (tid == 0) {
-        m.meta[s].osize = osize;
-        m.meta[s].csize = csize;
-        m.meta[s].comp = comp;
-        st_relaxed_u64(&flags[c], (c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
-        mbar_arrive(&m.sized[s]);
-      }
-
-      // ---- pack this chunk from registers --------------------------------------
-      if (comp) {
-        uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
-#pragma unroll
-        for (int u = 0; u < SPW; ++u) {
-          const int i = cw + u * ENC_CW;
-          const int wbase = __shfl_sync(0xffffffffu, incl - wc, i);
-          const int ln = __shfl_sync(0xffffffffu, ln_l, i);
-          pack_subchunk<T>(pw + wbase, ln, vals[u], lane);
-        }
-        if (cw == 0) {
-          stg[lane] = static_cast<uint8_t>(ln_l);
-          if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
+      if constexpr (KIND >= 0) {
+        compute_chunk<KIND>(stg, me, m, flags, cw, lane, tid);
+      } else {
+        switch (me.kind) {
+          case 0: compute_chunk<0>(stg, me, m, flags, cw, lane, tid); break;
+          case 1: compute_chunk<1>(stg, me, m, flags, cw, lane, tid); break;
+          case 2: compute_chunk<2>(stg, me, m, flags, cw, lane, tid); break;
+          default: compute_chunk<3>(stg, me, m, flags, cw, lane, tid); break;
         }
       }
-
       // ---- store the chunk of seq - 2 (its offset is known) ---------------------
       if (seq >= 2) store(seq - 2);
       fence_proxy_async_smem();  // generic accesses of this iteration before later TMA writes
@@ -405,17 +510,35 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const EncArgs a)
     }
   }
 
-  // ---- epilogue: the last CTA out writes the header and the stream size ------
+  // ---- epilogue: the last CTA out finishes the outputs -----------------------
   __syncthreads();
+  __shared__ int last_cta;
   if (tid == 0) {
     __threadfence();
     const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
-    if (d == gridDim.x - 1) {
-      __threadfence();
-      const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
-      const long long total = chunks ? static_cast<long long>(ld_relaxed_u64(&ws[WS_TOTAL])) : 0ll;
+    last_cta = d == gridDim.x - 1;
+    if (last_cta) __threadfence();
+  }
+  __syncthreads();
+  if (last_cta) {
+    const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+    if constexpr (BATCH) {
+      // buffers without chunks get their header-only stream; an error anywhere
+      // turns every size into -status
+      for (int i = tid; i < a.njobs; i += ENC_NT) {
+        const BatchJob& j = a.jobs[i];
+        if (st) {
+          *j.outsize = -static_cast<long long>(st);
+        } else if (j.chunks == 0) {
+          *reinterpret_cast<long long*>(j.out) = 0;
+          *j.outsize = 8;
+        }
+      }
+    } else if (tid == 0) {
+      const long long chunks = (a.insize + CS - 1) / CS;
+      const long long tot = chunks ? static_cast<long long>(ld_relaxed_u64(&ws[WS_TOTAL])) : 0ll;
       *reinterpret_cast<long long*>(a.out) = a.insize;
-      *a.outsize = st ? -static_cast<long long>(st) : 8 + 2 * chunks + total;
+      *a.outsize = st ? -static_cast<long long>(st) : 8 + 2 * chunks + tot;
     }
   }
 }
@@ -669,6 +792,293 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
 }
 
 // ============================================================================
+// batched decode: a prepass places every chunk, then a persistent kernel with a
+// producer warp and 8 compute warps decodes chunks in any order
+// ============================================================================
+constexpr int DB_STAGES = 4;
+constexpr int DB_CW = 8;
+constexpr int DB_NT = (DB_CW + 1) * 32;
+constexpr int DB_MINB = 3;
+
+struct DecBMeta {
+  long long g;      // chunk id across the launch, or NO_CHUNK
+  uint8_t* out;     // where the chunk's values go
+  QParams q;
+  int kind;         // bit 0: 64-bit values, bit 1: lossy
+  int osize;
+  int cs;
+  int sft;          // byte offset of the chunk within the staged copy
+  int state;        // 0: nothing to decode, 1: decode
+  int pad_;
+};
+
+struct DecBMisc {
+  uint64_t full[DB_STAGES];
+  uint64_t empty[DB_STAGES];
+  DecBMeta meta[DB_STAGES];
+  int lnv[SC];
+  int bitbase[SC];
+  int ok;
+};
+
+constexpr int DB_SMEM = DB_STAGES * STAGE_BYTES + ((sizeof(DecBMisc) + 127) / 128) * 128 + 8 * (BATCH_MAX_JOBS + 1);
+
+// Prepass, one CTA per buffer: validates the header and size table and writes the
+// byte offset of every chunk's payload (an exclusive scan of the sizes).
+__global__ void __launch_bounds__(256) k_decode_prepass(const BatchDecArgs a)
+{
+  __shared__ long long wsum[8];
+  __shared__ int wbad[8];
+  const int j = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const BatchJob& job = a.jobs[j];
+  const uint8_t* const in = job.in;
+  const long long len = job.insize;  // stream bytes, -1 when unknown
+  const int elem = (job.kind & 1) ? 8 : 4;
+  long long insize = (len < 0 || len >= 8) ? *reinterpret_cast<const long long*>(in) : -1;
+  bool ok = insize >= 0 && insize % elem == 0 && insize <= job.cap;
+  const long long chunks = ok ? (insize + CS - 1) / CS : 0;
+  if (ok && len >= 0 && 8 + 2 * chunks > len) ok = false;
+  if (!ok) {
+    if (tid == 0) set_status(a.ws, insize > job.cap ? ST_CAPACITY : ST_CORRUPT, j);
+    return;
+  }
+  const uint16_t* const size_in = reinterpret_cast<const uint16_t*>(in + 8);
+  long long* const offs = a.offsets + a.chunk_base[j];
+  long long carry = 0;
+  int bad = 0;
+  for (long long b = 0; b < chunks; b += 256) {
+    const long long c = b + tid;
+    int cs = 0;
+    if (c < chunks) {
+      cs = size_in[c];
+      const int os = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+      bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
+    }
+    long long incl = cs;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    long long before = carry;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    if (c < chunks) offs[c] = before + incl - cs;
+    long long tile = 0;
+    for (int w = 0; w < 8; ++w) tile += wsum[w];
+    carry += tile;
+    __syncthreads();
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) wbad[warp] = bad;
+  __syncthreads();
+  if (tid == 0) {
+    int any = 0;
+    for (int w = 0; w < 8; ++w) any |= wbad[w];
+    if (any || (len >= 0 && 8 + 2 * chunks + carry > len)) {
+      set_status(a.ws, ST_CORRUPT, j);
+    } else {
+      a.actual[j] = chunks;
+      a.actual_insize[j] = insize;
+      *job.outsize = insize;
+    }
+  }
+}
+
+// Decode one staged chunk (compute warps).
+template <int KIND>
+__device__ __forceinline__ void decode_chunk(const uint8_t* stg, const DecBMeta& d, DecBMisc& m, uint64_t* ws,
+                                             int cw, int lane, int tid)
+{
+  using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
+  constexpr bool LOSSY = (KIND & 2) != 0;
+  using V = VT<T>;
+  constexpr int NT = DB_CW * 32;
+  const int osize = d.osize;
+  T* const o = reinterpret_cast<T*>(d.out);
+  const int nv = osize / static_cast<int>(sizeof(T));
+  if (d.cs == osize) {  // raw chunk: shifted copy from the staged bytes
+    for (int e = tid; e < nv; e += NT) {
+      if constexpr (sizeof(T) == 4) o[e] = lds_u32_at_byte(stg, d.sft + 4 * e);
+      else o[e] = lds_u64_at_byte(stg, d.sft + 8 * e);
+    }
+    return;
+  }
+  if (cw == 0) {
+    const int ln = stg[d.sft + lane];
+    const int bitsw = ln * V::VPS;
+    int incl = bitsw;
+#pragma unroll
+    for (int k = 1; k < 32; k <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, k);
+      if (lane >= k) incl += t;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    m.lnv[lane] = ln;
+    m.bitbase[lane] = 8 * d.sft + 256 + incl - bitsw;
+    const bool bad_ln = __any_sync(0xffffffffu, ln > V::TB);
+    if (lane == 0) {
+      bool ok = !bad_ln && (34 + tot / 8 == d.cs);
+      if (ok) {
+        const int16_t tr = static_cast<int16_t>(stg[d.sft + d.cs - 2] | (stg[d.sft + d.cs - 1] << 8));
+        ok = tr == osize;
+      }
+      m.ok = ok;
+      if (!ok) set_status(ws, ST_CORRUPT, d.g);
+    }
+  }
+  cbar();
+  if (m.ok) {
+    const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
+    for (int k = tid; k < nv; k += NT) {
+      const int i = k / V::VPS;
+      const int jj = k - i * V::VPS;
+      const int ln = m.lnv[i];
+      T e = 0;
+      if (ln) {
+        if constexpr (sizeof(T) == 4) e = extract_bits32(w, m.bitbase[i] + jj * ln, ln);
+        else e = extract_bits64(w, m.bitbase[i] + jj * ln, ln);
+      }
+      o[k] = decode_value<LOSSY>(e, d.q);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(DB_NT, DB_MINB) k_decode_batch(const BatchDecArgs a)
+{
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t* const stage0 = smem;
+  DecBMisc& m = *reinterpret_cast<DecBMisc*>(smem + DB_STAGES * STAGE_BYTES);
+  long long* const cb = reinterpret_cast<long long*>(smem + DB_STAGES * STAGE_BYTES +
+                                                     ((sizeof(DecBMisc) + 127) / 128) * 128);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t* const ws = a.ws;
+  for (int i = tid; i <= a.njobs; i += DB_NT) cb[i] = a.chunk_base[i];
+  if (tid == 0) {
+    for (int s = 0; s < DB_STAGES; ++s) {
+      mbar_init(&m.full[s], 1);
+      mbar_init(&m.empty[s], 1);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const long long total = cb[a.njobs];
+  const bool failed_before = ld_relaxed_u64(&ws[WS_STATUS]) != 0ull;  // the prepass found an error
+
+  if (warp == DB_CW) {
+    // ===================== producer warp (lane 0 works, the warp follows) =====================
+    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
+    unsigned issued = 0, issued_par = 0;
+    for (int seq = 0;; ++seq) {
+      const int s = seq % DB_STAGES;
+      if (seq >= DB_STAGES) {
+        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - DB_STAGES) / DB_STAGES) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+          if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
+          break;
+        }
+      }
+      long long t = NO_CHUNK;
+      if (lane == 0 && !failed_before) t = static_cast<long long>(atomicAdd(tick, 1ull));
+      t = __shfl_sync(0xffffffffu, t, 0);
+      if (lane == 0) {
+        DecBMeta& d = m.meta[s];
+        bool copy = false;
+        if (t < total) {
+          int lo = 0, hi = a.njobs - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cb[mid] <= t) lo = mid;
+            else hi = mid - 1;
+          }
+          const BatchJob& job = a.jobs[lo];
+          const long long c = t - cb[lo];
+          const long long chunks = a.actual[lo];
+          d.g = t;
+          d.state = 0;
+          if (c < chunks) {
+            const long long insize = a.actual_insize[lo];
+            const uint8_t* const data_in = job.in + 8 + 2 * chunks;
+            const long long off = a.offsets[t];
+            const int cs = reinterpret_cast<const uint16_t*>(job.in + 8)[c];
+            const uint8_t* const src = data_in + off;
+            const int sft = static_cast<int>(reinterpret_cast<uintptr_t>(src) & 15u);
+            d.out = job.out + c * CS;
+            d.q = job.q;
+            d.kind = job.kind;
+            d.osize = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+            d.cs = cs;
+            d.sft = sft;
+            d.state = 1;
+            const uint32_t nb = static_cast<uint32_t>((sft + cs + 15) & ~15);
+            mbar_arrive_expect_tx(&m.full[s], nb);
+            tma_load_1d(stage0 + s * STAGE_BYTES, src - sft, nb, &m.full[s]);
+            copy = true;
+          }
+        } else {
+          d.g = NO_CHUNK;
+        }
+        if (copy) {
+          issued |= 1u << s;
+          issued_par = (issued_par & ~(1u << s)) | (((seq / DB_STAGES) & 1u) << s);
+        } else {
+          issued &= ~(1u << s);
+          mbar_arrive(&m.full[s]);
+        }
+      }
+      __syncwarp();
+      if (t >= total) break;
+    }
+    if (lane == 0) {
+      for (int s = 0; s < DB_STAGES; ++s)
+        if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
+    }
+  } else {
+    // ===================== compute warps =====================
+    for (int seq = 0;; ++seq) {
+      const int s = seq % DB_STAGES;
+      const bool ok = mbar_wait_bounded(&m.full[s], (seq / DB_STAGES) & 1);
+      if (cbar_or(!ok)) {
+        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+        break;
+      }
+      const DecBMeta& d = m.meta[s];
+      if (d.g == NO_CHUNK) break;
+      if (d.state == 1) {
+        const uint8_t* const stg = stage0 + s * STAGE_BYTES;
+        switch (d.kind) {
+          case 0: decode_chunk<0>(stg, d, m, ws, warp, lane, tid); break;
+          case 1: decode_chunk<1>(stg, d, m, ws, warp, lane, tid); break;
+          case 2: decode_chunk<2>(stg, d, m, ws, warp, lane, tid); break;
+          default: decode_chunk<3>(stg, d, m, ws, warp, lane, tid); break;
+        }
+      }
+      fence_proxy_async_smem();
+      cbar();
+      if (tid == 0) mbar_arrive(&m.empty[s]);
+    }
+  }
+
+  // ---- epilogue: an error anywhere turns every size into -status ---------------
+  __syncthreads();
+  __shared__ int last_cta;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
+    last_cta = dn == gridDim.x - 1;
+    if (last_cta) __threadfence();
+  }
+  __syncthreads();
+  if (last_cta) {
+    const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+    if (st)
+      for (int i = tid; i < a.njobs; i += DB_NT) *a.jobs[i].outsize = -static_cast<long long>(st);
+  }
+}
+
+// ============================================================================
 // launchers
 // ============================================================================
 // Sets the dynamic shared memory limit of `k` once per device.
@@ -688,7 +1098,7 @@ static cudaError_t ensure_smem_attr(K k, int bytes, unsigned long long* done_mas
 template <typename T, bool LOSSY>
 static cudaError_t launch_encode_t(const EncArgs& a, int grid, cudaStream_t st)
 {
-  auto k = k_encode<T, LOSSY, ENC_MINB>;
+  auto k = k_encode<(sizeof(T) == 8 ? 1 : 0) | (LOSSY ? 2 : 0), false, ENC_MINB>;
   static unsigned long long attr = 0;
   cudaError_t e = ensure_smem_attr(k, ENC_SMEM, &attr);
   if (e != cudaSuccess) return e;
@@ -712,7 +1122,7 @@ template <typename T, bool LOSSY>
 static int occupancy_t(bool enc)
 {
   int n = 0;
-  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<T, LOSSY, ENC_MINB>, ENC_NT, ENC_SMEM);
+  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<(sizeof(T) == 8 ? 1 : 0) | (LOSSY ? 2 : 0), false, ENC_MINB>, ENC_NT, ENC_SMEM);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decode<T, LOSSY, 256, 4>, 256, DEC_SMEM);
   return n;
 }
@@ -721,6 +1131,44 @@ cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cud
 {
   if (width == 4) return lossy ? launch_encode_t<uint32_t, true>(a, grid, st) : launch_encode_t<uint32_t, false>(a, grid, st);
   return lossy ? launch_encode_t<uint64_t, true>(a, grid, st) : launch_encode_t<uint64_t, false>(a, grid, st);
+}
+
+cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st)
+{
+  auto k = k_encode<-1, true, ENC_MINB>;
+  static unsigned long long attr = 0;
+  cudaError_t e = ensure_smem_attr(k, ENC_BATCH_SMEM, &attr);
+  if (e != cudaSuccess) return e;
+  k<<<grid, ENC_NT, ENC_BATCH_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decode_batch(const BatchDecArgs& a, int grid, cudaStream_t st)
+{
+  k_decode_prepass<<<a.njobs, 256, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  static unsigned long long attr = 0;
+  e = ensure_smem_attr(k_decode_batch, DB_SMEM, &attr);
+  if (e != cudaSuccess) return e;
+  k_decode_batch<<<grid, DB_NT, DB_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+int decode_batch_blocks_per_sm()
+{
+  cudaFuncSetAttribute(k_decode_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, DB_SMEM);
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decode_batch, DB_NT, DB_SMEM);
+  return n;
+}
+
+int encode_batch_blocks_per_sm()
+{
+  cudaFuncSetAttribute(k_encode<-1, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_BATCH_SMEM);
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<-1, true, ENC_MINB>, ENC_NT, ENC_BATCH_SMEM);
+  return n;
 }
 
 cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st)
@@ -734,20 +1182,20 @@ int blocks_per_sm(int width, bool lossy, bool enc)
   // the smem attribute must be set before the occupancy query counts dynamic smem
   if (width == 4) {
     if (lossy) {
-      cudaFuncSetAttribute(k_encode<uint32_t, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+      cudaFuncSetAttribute(k_encode<2, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
       cudaFuncSetAttribute(k_decode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
       return occupancy_t<uint32_t, true>(enc);
     }
-    cudaFuncSetAttribute(k_encode<uint32_t, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_encode<0, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
     cudaFuncSetAttribute(k_decode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
     return occupancy_t<uint32_t, false>(enc);
   }
   if (lossy) {
-    cudaFuncSetAttribute(k_encode<uint64_t, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+    cudaFuncSetAttribute(k_encode<3, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
     cudaFuncSetAttribute(k_decode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
     return occupancy_t<uint64_t, true>(enc);
   }
-  cudaFuncSetAttribute(k_encode<uint64_t, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
+  cudaFuncSetAttribute(k_encode<1, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
   cudaFuncSetAttribute(k_decode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
   return occupancy_t<uint64_t, false>(enc);
 }

@@ -36,7 +36,43 @@ struct DecArgs {
   QParams q;
 };
 
+// One buffer of a batched launch (device table entry).
+struct BatchJob {
+  const uint8_t* in;     // compress: values; decompress: stream
+  uint8_t* out;          // compress: stream; decompress: values
+  long long* outsize;    // device: bytes written, or -status
+  long long insize;      // compress: input bytes; decompress: stream bytes (-1 = unknown)
+  long long cap;         // decompress: output capacity in bytes
+  long long chunks;      // compress: chunks; decompress: chunks the capacity allows
+  QParams q;
+  int kind;              // bit 0: 64-bit values, bit 1: lossy
+  int pad_;
+};
+
+constexpr int BATCH_MAX_JOBS = 1024;  // buffers per launch (the chunk table lives in shared memory)
+
+struct BatchEncArgs {
+  const BatchJob* jobs;         // device table
+  const long long* chunk_base;  // device: first chunk id of each job, then the total (njobs + 1)
+  int njobs;
+  uint64_t* ws;                 // zeroed workspace: header words + one flag per chunk
+};
+
+struct BatchDecArgs {
+  const BatchJob* jobs;         // device table (in: stream, insize: stream bytes or -1, cap: output bytes)
+  const long long* chunk_base;  // device: first chunk id of each job by capacity, then the total
+  int njobs;
+  uint64_t* ws;                 // zeroed workspace header words
+  long long* offsets;           // workspace: payload offset of every chunk id
+  long long* actual;            // workspace: chunks in each stream (from its header)
+  long long* actual_insize;     // workspace: bytes each stream decodes to
+};
+
 cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_decode_batch(const BatchDecArgs& a, int grid, cudaStream_t st);
+int decode_batch_blocks_per_sm();
+cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st);
+int encode_batch_blocks_per_sm();
 cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st);
 int blocks_per_sm(int width, bool lossy, bool enc);
 
