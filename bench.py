@@ -214,6 +214,114 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def bench_batched(dev, world, args):
+    """The batched workload (1000 arrays, 4 KB - 64 MB, mixed dtypes and bounds):
+    one graph-captured persistent launch vs 1000 sequential plain launches (also
+    graph-captured, so host launch overhead is not counted against the plain
+    form), with every stream and decoded array compared bit for bit."""
+    from sleek_b200 import _capi, api, autotune, workloads
+    from sleek_b200.batch import BatchPlan
+
+    L = _capi.lib()
+    arrays, ebs = workloads.batched_arrays(1000, device=dev)
+    total = sum(a.numel() * a.element_size() for a in arrays)
+    st = torch.cuda.current_stream()
+
+    # sequential plain launches through the C ABI, one buffer per call
+    outs = [torch.empty(api.sleek_upper_bound_size(a.numel() * a.element_size()) + 16, dtype=torch.uint8,
+                        device=dev) for a in arrays]
+    szs = torch.zeros(len(arrays), dtype=torch.int64, device=dev)
+    wsb = max(L.sleek_compress_workspace_size(a.numel() * a.element_size()) for a in arrays)
+    wsb = max(wsb, L.sleek_decompress_workspace_size())
+    ws = torch.zeros(wsb, dtype=torch.uint8, device=dev)
+    ebi = [None if eb is None else api.sleek_error_bound(eb, np.float32 if a.dtype == torch.float32
+                                                         else np.float64).c_struct() for a, eb in zip(arrays, ebs)]
+
+    def seq_compress(stream):
+        sh = stream.cuda_stream
+        for i, a in enumerate(arrays):
+            t = "f32" if a.dtype == torch.float32 else "f64"
+            if ebi[i] is None:
+                rc = getattr(L, f"sleek_compress_{t}")(a.data_ptr(), a.numel(), outs[i].data_ptr(),
+                                                       szs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+            else:
+                rc = getattr(L, f"sleek_compress_lossy_{t}")(ebi[i], a.data_ptr(), a.numel(), outs[i].data_ptr(),
+                                                             szs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+            _capi.check(rc)
+
+    decs = [torch.empty_like(a) for a in arrays]
+    dszs = torch.zeros(len(arrays), dtype=torch.int64, device=dev)
+
+    def seq_decompress(stream):
+        sh = stream.cuda_stream
+        for i, a in enumerate(arrays):
+            t = "f32" if a.dtype == torch.float32 else "f64"
+            cap = a.numel() * a.element_size()
+            if ebi[i] is None:
+                rc = getattr(L, f"sleek_decompress_{t}")(outs[i].data_ptr(), outs[i].numel(), decs[i].data_ptr(), cap,
+                                                         dszs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+            else:
+                rc = getattr(L, f"sleek_decompress_lossy_{t}")(ebi[i], outs[i].data_ptr(), outs[i].numel(),
+                                                               decs[i].data_ptr(), cap, dszs[i:].data_ptr(),
+                                                               ws.data_ptr(), wsb, sh)
+            _capi.check(rc)
+
+    def graph_of(fn):
+        fn(st)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s2 = torch.cuda.Stream()
+        s2.wait_stream(st)
+        with torch.cuda.stream(s2):
+            with torch.cuda.graph(g, stream=s2):
+                fn(s2)
+        st.wait_stream(s2)
+        return g
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    g_seq_c = graph_of(seq_compress)
+    t_seq_c = timed(g_seq_c.replay)
+    g_seq_d = graph_of(seq_decompress)
+    t_seq_d = timed(g_seq_d.replay)
+
+    plan = BatchPlan.compress(arrays, ebs)
+    tuned_c = autotune.tune_plan(plan, f"c3-compress-{len(arrays)}", use_cache=False)
+    t_bat_c = timed(plan.graph().replay)
+    seq_sizes = szs.cpu().tolist()
+    bat_streams = plan.streams()
+    exact = all(int(n) == s.numel() and torch.equal(o[:int(n)], s)
+                for o, n, s in zip(outs, seq_sizes, bat_streams))
+    dplan = BatchPlan.decompress(bat_streams, [np.float32 if a.dtype == torch.float32 else np.float64
+                                               for a in arrays], ebs,
+                                 num_elements=[a.numel() for a in arrays])
+    tuned_d = autotune.tune_plan(dplan, f"c3-decompress-{len(arrays)}", use_cache=False)
+    t_bat_d = timed(dplan.graph().replay)
+    exact = exact and all(torch.equal(d.view(torch.int32 if d.dtype == torch.float32 else torch.int64),
+                                      o.view(torch.int32 if o.dtype == torch.float32 else torch.int64))
+                          for d, o in zip(decs, dplan.arrays()))
+    gbs = lambda ms: round(total / (ms * 1e-3) / 1e9, 1)
+    return {
+        "workload": "1000 arrays, log-uniform 4 KB-64 MB, f32/f64, half lossless / half lossy eb in [1e-6,1e-1]",
+        "total_bytes": total,
+        "compress_gbs": {"batched_graph": gbs(t_bat_c), "sequential_plain_graph": gbs(t_seq_c),
+                         "speedup": round(t_seq_c / t_bat_c, 2)},
+        "decompress_gbs": {"batched_graph": gbs(t_bat_d), "sequential_plain_graph": gbs(t_seq_d),
+                           "speedup": round(t_seq_d / t_bat_d, 2)},
+        "autotuned_ctas_per_sm": {"compress": tuned_c["best"], "decompress": tuned_d["best"]},
+        "bit_exact_vs_plain": bool(exact),
+    }
+
+
 def config_dict(args):
     return {"workload": "c1 f64 turbulence field 256x384x384 (301,989,888 B), lossless + eb 1e-2/1e-4/1e-6, "
                         "compress+decompress per mode",
@@ -234,6 +342,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (1000-array) comparison")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -429,6 +538,11 @@ def main():
         "gpu_launches": 2 * len(MODES) * args.steps,
         "clocks": clocks,
     }
+    if not args.no_batched:
+        # free the single-buffer leg's buffers first
+        del enc, dec, d_in, d_enc, hin, hout, hstream
+        torch.cuda.empty_cache()
+        line["batched"] = bench_batched(dev, world, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
     if rank == 0:

@@ -129,6 +129,11 @@ int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* d_enco
 int sleek_compress_f32_static(const float* d_input, long long num_elements, unsigned char* d_encoded,
                               long long* d_encsize, void* stream);
 
+/* Tuning: CTAs per SM used by the single-buffer entry points of one kind on the current
+ * device (0 = as many as fit, the default).  Set by sleek_b200.autotune; no counterpart
+ * in the reference, whose grid size comes from sleek_thread_blocks. */
+int sleek_set_ctas_per_sm(int decompress, int elem_bytes, int lossy, int ctas_per_sm);
+
 /* ---- batched compress / decompress ---------------------------------------------
  * Many buffers of uneven sizes with mixed float32 / float64 and mixed error bounds in
  * one persistent launch (per group of up to 1024 buffers).  The batched form has no

@@ -21,7 +21,8 @@ constexpr int HDR_WORDS = 32;  // workspace header words, as in sleek_device.cuh
 
 struct DeviceInfo {
   int sms = 0;
-  int bps[2][2][2] = {};  // [width==8][lossy][enc]
+  int bps[2][2][2] = {};       // [width==8][lossy][enc]: CTAs per SM that fit
+  int override_[2][2][2] = {};  // tuned CTAs per SM (0 = as many as fit)
 };
 
 std::mutex g_mu;
@@ -51,7 +52,8 @@ int persistent_grid(int dev, int width, bool lossy, bool enc)
     const int n = sleek::blocks_per_sm(width, lossy, enc);
     b = n > 0 ? n : 1;
   }
-  return d.sms * b;
+  const int o = d.override_[width == 8][lossy][enc];
+  return d.sms * ((o > 0 && o < b) ? o : b);
 }
 
 // library-owned workspace for (device, stream); grows, never shrinks
@@ -320,6 +322,17 @@ int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* in, lo
 {
   if (eb.thr_e != eb.eb_e + 53 || eb.thr_e >= 2047 || eb.eb_e < 0) return SLEEK_ERR_ERROR_BOUND;
   return do_decompress(8, true, qp(eb.eb_e, eb.thr_e, eb.offs_e), in, in_len, out, cap, outsize, ws, wsb, stream);
+}
+
+int sleek_set_ctas_per_sm(int decompress, int elem_bytes, int lossy, int ctas_per_sm)
+{
+  if ((elem_bytes != 4 && elem_bytes != 8) || ctas_per_sm < 0) return SLEEK_ERR_INVALID_ARG;
+  int dev = 0;
+  const int rc = current_device(&dev);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_dev[dev].override_[elem_bytes == 8][lossy != 0][decompress == 0] = ctas_per_sm;
+  return SLEEK_OK;
 }
 
 int sleek_workspace_status(const void* ws, void* stream, int* status)

@@ -162,3 +162,21 @@ def _fit(f: torch.Tensor, n: int) -> torch.Tensor:
         return f[:n].contiguous()
     reps = (n + f.numel() - 1) // f.numel()
     return f.repeat(reps)[:n].contiguous()
+
+
+def batched_arrays(n: int = 1000, variant: int = 0, device="cpu", min_bytes: int = 4096,
+                   max_bytes: int = 64 << 20):
+    """The batched workload: n arrays with sizes log-uniform in [min_bytes, max_bytes]
+    (rounded down to the element size), float32 / float64 by a fair coin, generators
+    c0 / c1 / c2 in turn; even-index arrays lossless, odd ones lossy with bounds
+    log-uniform in [1e-6, 1e-1].  Returns (arrays, error_bounds)."""
+    rng = np.random.default_rng(seed_of(3, variant))
+    arrays, ebs = [], []
+    fams = ("c0", "c1", "c2")
+    for i in range(n):
+        nbytes = int(np.exp(rng.uniform(np.log(min_bytes), np.log(max_bytes))))
+        dt = torch.float32 if rng.random() < 0.5 else torch.float64
+        x = scaled(fams[i % 3], nbytes, device=device, dtype=dt, variant=i)
+        arrays.append(x)
+        ebs.append(None if i % 2 == 0 else float(10 ** rng.uniform(-6, -1)))
+    return arrays, ebs
