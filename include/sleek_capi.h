@@ -156,6 +156,13 @@ typedef struct sleek_batch_plan sleek_batch_plan;
 /* Validates the items, derives the quantizer parameters and uploads the job tables
  * (allocates device memory and synchronises: call it outside stream capture). */
 int sleek_batch_plan_create(const sleek_batch_item* items, int n, int decompress, sleek_batch_plan** plan);
+/* A reusable plan with room for `capacity` items (at most 1024): device tables and a
+ * pinned staging area are allocated once, then sleek_batch_plan_set_items replaces the
+ * item list with an asynchronous upload on `stream` (no allocation, no host wait), so a
+ * serving loop can launch batch after batch.  Call set_items again only after the
+ * previous run of the same plan has completed (the staging area is reused). */
+int sleek_batch_plan_create_reusable(int capacity, int decompress, sleek_batch_plan** plan);
+int sleek_batch_plan_set_items(sleek_batch_plan* plan, const sleek_batch_item* items, int n, void* stream);
 /* Workspace bytes a run of the plan needs. */
 size_t sleek_batch_plan_workspace_size(const sleek_batch_plan* plan);
 /* Tuning: CTAs per SM of the plan's launches (0 = as many as fit). */

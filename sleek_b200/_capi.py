@@ -67,6 +67,8 @@ SIGNATURES = {
     "sleek_set_ctas_per_sm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
     "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "sleek_batch_plan_workspace_size": (_sz, [_vp]),
+    "sleek_batch_plan_create_reusable": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "sleek_batch_plan_set_items": (C.c_int, [_vp, C.c_void_p, C.c_int, _vp]),
     "sleek_batch_plan_set_grid": (C.c_int, [_vp, C.c_int]),
     "sleek_batch_plan_run": (C.c_int, [_vp, _vp, _sz, _vp]),
     "sleek_batch_plan_destroy": (C.c_int, [_vp]),

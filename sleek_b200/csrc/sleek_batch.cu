@@ -38,6 +38,10 @@ struct sleek_batch_plan {
   int grid_scale = 0;  // CTAs per SM; 0 = as many as fit
   std::vector<Group> groups;
   size_t ws_bytes = 0;
+  // reusable plans: one group whose tables are refilled from pinned staging
+  int capacity = 0;
+  sleek::BatchJob* h_jobs = nullptr;
+  long long* h_cb = nullptr;
 };
 
 namespace {
@@ -95,6 +99,8 @@ void free_plan(sleek_batch_plan* p)
     if (g.d_jobs) cudaFree(g.d_jobs);
     if (g.d_cb) cudaFree(g.d_cb);
   }
+  if (p->h_jobs) cudaFreeHost(p->h_jobs);
+  if (p->h_cb) cudaFreeHost(p->h_cb);
   delete p;
 }
 
@@ -163,6 +169,62 @@ int sleek_batch_plan_create(const sleek_batch_item* items, int n, int decompress
   return SLEEK_OK;
 }
 
+int sleek_batch_plan_create_reusable(int capacity, int decompress, sleek_batch_plan** plan)
+{
+  if (!plan || capacity < 1 || capacity > sleek::BATCH_MAX_JOBS) return SLEEK_ERR_INVALID_ARG;
+  *plan = nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SLEEK_ERR_NO_DEVICE;
+  }
+  sleek_batch_plan* p = new (std::nothrow) sleek_batch_plan();
+  if (!p) return SLEEK_ERR_INVALID_ARG;
+  p->decompress = decompress ? 1 : 0;
+  p->device = dev;
+  p->capacity = capacity;
+  Group g;
+  if (cudaMalloc(&g.d_jobs, sizeof(sleek::BatchJob) * capacity) != cudaSuccess ||
+      cudaMalloc(&g.d_cb, sizeof(long long) * (capacity + 1)) != cudaSuccess ||
+      cudaMallocHost(&p->h_jobs, sizeof(sleek::BatchJob) * capacity) != cudaSuccess ||
+      cudaMallocHost(&p->h_cb, sizeof(long long) * (capacity + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    p->groups.push_back(g);
+    free_plan(p);
+    return SLEEK_ERR_CUDA;
+  }
+  p->groups.push_back(g);
+  *plan = p;
+  return SLEEK_OK;
+}
+
+int sleek_batch_plan_set_items(sleek_batch_plan* plan, const sleek_batch_item* items, int n, void* stream)
+{
+  if (!plan || plan->capacity == 0 || n < 0 || n > plan->capacity || (n > 0 && !items)) return SLEEK_ERR_INVALID_ARG;
+  Group& g = plan->groups[0];
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    const int rc = fill_job(items[i], plan->decompress, plan->h_jobs[i]);
+    if (rc) return rc;
+    plan->h_cb[i] = total;
+    total += plan->h_jobs[i].chunks;
+  }
+  plan->h_cb[n] = total;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((n > 0 && cudaMemcpyAsync(g.d_jobs, plan->h_jobs, sizeof(sleek::BatchJob) * n, cudaMemcpyHostToDevice, st) !=
+                    cudaSuccess) ||
+      cudaMemcpyAsync(g.d_cb, plan->h_cb, sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    cudaGetLastError();
+    return SLEEK_ERR_CUDA;
+  }
+  g.njobs = n;
+  g.chunks = total;
+  g.ws_bytes = plan->decompress ? static_cast<size_t>(8 * (HDR_WORDS + total + 2 * n))
+                                : static_cast<size_t>(8 * (HDR_WORDS + total));
+  plan->ws_bytes = g.ws_bytes;
+  return SLEEK_OK;
+}
+
 size_t sleek_batch_plan_workspace_size(const sleek_batch_plan* plan) { return plan ? plan->ws_bytes : 0; }
 
 int sleek_batch_plan_set_grid(sleek_batch_plan* plan, int ctas_per_sm)
@@ -180,6 +242,7 @@ int sleek_batch_plan_run(sleek_batch_plan* plan, void* d_workspace, size_t works
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   uint64_t* const ws = static_cast<uint64_t*>(d_workspace);
   for (const Group& g : plan->groups) {
+    if (g.njobs == 0) continue;
     if (cudaMemsetAsync(ws, 0, g.ws_bytes, st) != cudaSuccess) {
       cudaGetLastError();
       return SLEEK_ERR_CUDA;

@@ -1,0 +1,278 @@
+"""Serving loop: compress / decompress requests of different sizes, taken as they
+arrive and run with continuous batching.
+
+- Outputs live in one device-resident arena (``DevicePool``, first-fit with
+  coalescing): a request is admitted only when its output fits in free HBM, and
+  its memory returns to the pool when it completes.
+- ``slots`` CUDA streams each own a reusable compress plan and a reusable
+  decompress plan (``sleek_batch_plan_set_items``: no allocation per batch).  Any
+  idle slot takes every admitted request waiting at that moment (up to the plan
+  capacity and workspace), so requests that arrive while others are on the GPU
+  join the next launch, and launches on different slots overlap on the device.
+- Latency is measured from a request's arrival to the host seeing its batch
+  complete; ``stats`` reports p50 / p99 and aggregate GB/s of uncompressed bytes.
+
+Every request's result is bit-identical to running it alone through the
+single-buffer entry points (the batched kernels produce the same streams).
+"""
+from __future__ import annotations
+
+import bisect
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _capi
+from .api import sleek_upper_bound_size
+
+GRANULE = 256
+ITEM_DTYPE = np.dtype([("input", np.uint64), ("output", np.uint64), ("size_out", np.uint64),
+                       ("num_elements", np.int64), ("stream_bytes", np.int64), ("elem_bytes", np.int32),
+                       ("lossy", np.int32), ("error_bound", np.float64)])
+assert ITEM_DTYPE.itemsize == 56  # sleek_batch_item
+
+
+class DevicePool:
+    """First-fit allocator over one device arena; free ranges are coalesced."""
+
+    def __init__(self, nbytes: int, device="cuda"):
+        nbytes = (nbytes // GRANULE) * GRANULE
+        self.arena = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        self.base = self.arena.data_ptr()
+        self.size = nbytes
+        self._starts = [0]          # sorted free range starts
+        self._ends = {0: nbytes}    # start -> end
+        self.free_bytes = nbytes
+
+    def alloc(self, n: int) -> Optional[int]:
+        n = max(GRANULE, (n + GRANULE - 1) // GRANULE * GRANULE)
+        for i, s in enumerate(self._starts):
+            e = self._ends[s]
+            if e - s >= n:
+                del self._ends[s]
+                self._starts.pop(i)
+                if e - s > n:
+                    bisect.insort(self._starts, s + n)
+                    self._ends[s + n] = e
+                self.free_bytes -= n
+                return s
+        return None
+
+    def free(self, off: int, n: int) -> None:
+        n = max(GRANULE, (n + GRANULE - 1) // GRANULE * GRANULE)
+        s, e = off, off + n
+        i = bisect.bisect_left(self._starts, s)
+        if i < len(self._starts) and self._starts[i] == e:  # merge with the next range
+            e = self._ends.pop(e)
+            self._starts.pop(i)
+        if i > 0 and self._ends[self._starts[i - 1]] == s:  # merge with the previous range
+            s = self._starts[i - 1]
+            self._ends[s] = e
+        else:
+            self._starts.insert(i, s)
+            self._ends[s] = e
+        self.free_bytes += n
+
+    def view(self, off: int, n: int) -> torch.Tensor:
+        return self.arena[off:off + n]
+
+
+@dataclass
+class Request:
+    op: str                     # "compress" or "decompress"
+    src: torch.Tensor           # compress: device values; decompress: device stream (uint8)
+    dtype: np.dtype
+    eb: Optional[float] = None
+    num_elements: int = 0       # decompress: elements the stream decodes to
+    arrival: float = 0.0        # seconds, on the server's clock
+    rid: int = 0
+    # filled by the server
+    out_off: int = -1
+    out_bytes: int = 0
+    done: float = -1.0
+    result_bytes: int = -1
+
+    @property
+    def raw_bytes(self) -> int:
+        if self.op == "compress":
+            return self.src.numel() * self.src.element_size()
+        return self.num_elements * np.dtype(self.dtype).itemsize
+
+
+@dataclass
+class _Slot:
+    stream: torch.cuda.Stream
+    plans: dict
+    ws: dict
+    sizes: torch.Tensor
+    busy: bool = False
+    event: Optional[torch.cuda.Event] = None
+    reqs: List[Request] = field(default_factory=list)
+
+
+class Server:
+    def __init__(self, hbm_budget: int, slots: int = 4, max_batch: int = 512, max_batch_chunks: int = 1 << 16,
+                 device="cuda"):
+        self.pool = DevicePool(hbm_budget, device)
+        self.max_batch = max_batch
+        self.max_batch_chunks = max_batch_chunks
+        L = _capi.lib()
+        self._L = L
+        self.slots: List[_Slot] = []
+        for _ in range(slots):
+            plans = {}
+            for op, dec in (("compress", 0), ("decompress", 1)):
+                h = _capi.C.c_void_p()
+                _capi.check(L.sleek_batch_plan_create_reusable(max_batch, dec, _capi.C.byref(h)))
+                plans[op] = h
+            ws = {op: torch.zeros(8 * (32 + max_batch_chunks + 2 * max_batch), dtype=torch.uint8, device=device)
+                  for op in ("compress", "decompress")}
+            self.slots.append(_Slot(torch.cuda.Stream(device=device), plans, ws,
+                                    torch.zeros(2 * max_batch, dtype=torch.int64, device=device)))
+        self.queue: List[Request] = []
+        self.completed: List[Request] = []
+        self.t0 = time.perf_counter()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    # ---- admission and dispatch ----------------------------------------------------------
+    def submit(self, r: Request) -> None:
+        self.queue.append(r)
+
+    def _out_bytes(self, r: Request) -> int:
+        if r.op == "compress":
+            return sleek_upper_bound_size(r.raw_bytes)
+        return r.raw_bytes
+
+    def _take(self) -> List[Request]:
+        """Admitted requests for one launch: outputs allocated from the pool, in
+        arrival order, skipping (for now) those that do not fit yet."""
+        take, chunks, keep = [], 0, []
+        for r in self.queue:
+            ch = (r.raw_bytes + 16383) // 16384
+            if len(take) < self.max_batch and chunks + ch <= self.max_batch_chunks:
+                n = self._out_bytes(r)
+                off = self.pool.alloc(n)
+                if off is not None:
+                    r.out_off, r.out_bytes = off, n
+                    take.append(r)
+                    chunks += ch
+                    continue
+            keep.append(r)
+        self.queue = keep
+        return take
+
+    def _launch(self, slot: _Slot, reqs: List[Request]) -> None:
+        slot.reqs = reqs
+        slot.busy = True
+        k = 0
+        with torch.cuda.stream(slot.stream):
+            for op in ("compress", "decompress"):
+                part = [r for r in reqs if r.op == op]
+                if not part:
+                    continue
+                items = np.zeros(len(part), ITEM_DTYPE)
+                comp = op == "compress"
+                items["input"] = [r.src.data_ptr() for r in part]
+                items["output"] = [self.pool.base + r.out_off for r in part]
+                items["size_out"] = slot.sizes.data_ptr() + 8 * (k + np.arange(len(part), dtype=np.uint64))
+                items["num_elements"] = [r.src.numel() if comp else r.num_elements for r in part]
+                items["stream_bytes"] = [-1 if comp else r.src.numel() for r in part]
+                items["elem_bytes"] = [np.dtype(r.dtype).itemsize for r in part]
+                items["lossy"] = [int(r.eb is not None) for r in part]
+                items["error_bound"] = [float(r.eb) if r.eb is not None else 0.0 for r in part]
+                h = slot.plans[op]
+                sh = slot.stream.cuda_stream
+                _capi.check(self._L.sleek_batch_plan_set_items(h, items.ctypes.data, len(part), sh))
+                ws = slot.ws[op]
+                _capi.check(self._L.sleek_batch_plan_run(h, ws.data_ptr(), ws.numel(), sh))
+                for i, r in enumerate(part):
+                    r._slot_index = k + i
+                k += len(part)
+            slot.event = torch.cuda.Event()
+            slot.event.record(slot.stream)
+
+    def poll(self) -> int:
+        """Completes finished launches; returns how many requests completed."""
+        n = 0
+        for slot in self.slots:
+            if slot.busy and slot.event.query():
+                sizes = slot.sizes[: len(slot.reqs)].cpu().tolist() if slot.reqs else []
+                t = self.now()
+                for r in slot.reqs:
+                    r.done = t
+                    r.result_bytes = int(sizes[r._slot_index])
+                    self.completed.append(r)
+                n += len(slot.reqs)
+                slot.busy = False
+                slot.reqs = []
+        return n
+
+    def dispatch(self) -> None:
+        for slot in self.slots:
+            if not self.queue:
+                return
+            if not slot.busy:
+                reqs = self._take()
+                if reqs:
+                    self._launch(slot, reqs)
+
+    def result(self, r: Request) -> torch.Tensor:
+        """A completed request's output (a view into the pool until released)."""
+        if r.result_bytes < 0:
+            raise _capi.SleekError(-r.result_bytes, "serve")
+        return self.pool.view(r.out_off, r.result_bytes)
+
+    def release(self, r: Request) -> None:
+        if r.out_off >= 0:
+            self.pool.free(r.out_off, r.out_bytes)
+            r.out_off = -1
+
+    # ---- driving a workload --------------------------------------------------------------
+    def serve(self, requests: List[Request], keep=None) -> dict:
+        """Feeds requests at their arrival times (seconds from now) and runs until all
+        complete.  Outputs are released on completion unless ``keep(r)`` is true."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        self.t0 = time.perf_counter()
+        self.completed = []
+        i = 0
+        while i < len(pending) or self.queue or any(s.busy for s in self.slots):
+            t = self.now()
+            while i < len(pending) and pending[i].arrival <= t:
+                self.submit(pending[i])
+                i += 1
+            done_before = len(self.completed)
+            self.poll()
+            for r in self.completed[done_before:]:
+                if keep is None or not keep(r):
+                    self.release(r)
+            self.dispatch()
+        for s in self.slots:
+            s.stream.synchronize()
+        return self.stats()
+
+    def stats(self) -> dict:
+        lat = np.array([r.done - r.arrival for r in self.completed]) * 1e3
+        span = max(r.done for r in self.completed) - min(r.arrival for r in self.completed)
+        nbytes = sum(r.raw_bytes for r in self.completed)
+        return {"requests": len(self.completed), "bytes": nbytes, "span_s": round(span, 4),
+                "gbs": round(nbytes / span / 1e9, 1) if span > 0 else None,
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "errors": sum(1 for r in self.completed if r.result_bytes < 0)}
+
+    def close(self) -> None:
+        for s in self.slots:
+            s.stream.synchronize()
+            for h in s.plans.values():
+                self._L.sleek_batch_plan_destroy(h)
+            s.plans = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
