@@ -322,6 +322,78 @@ def bench_batched(dev, world, args):
     }
 
 
+def bench_serve(dev, n_requests: int, seed: int = 4):
+    """The served workload: Poisson arrivals at 70 % of the loop's measured peak,
+    sizes log-uniform 1 KB - 256 MB, 60 / 40 compress / decompress, half lossy with
+    bounds log-uniform in [1e-6, 1e-2], outputs in a device pool of up to 150 GB.
+    Decompress requests read streams made beforehand by the compressor (equal to
+    the oracle's by the parity tests).  1 % of the requests are re-run alone
+    through the single-buffer entry points and compared bit for bit."""
+    from sleek_b200 import api
+    from sleek_b200.serve import Request, Server
+
+    rng = np.random.default_rng(20261203 + 4000 + seed)
+    n_src = 1 << 31  # 8 GB of f32 + 8 GB of f64 source values
+    g = torch.Generator(device=dev).manual_seed(20261203 + 4000)
+    src32 = (torch.cumsum(torch.randn(n_src // 4, generator=g, device=dev), 0) * 1e-3).contiguous()
+    src64 = (torch.cumsum(torch.randn(n_src // 8, generator=g, device=dev, dtype=torch.float64), 0) * 1e-3)
+    lo, hi = np.log(1024), np.log(256 << 20)
+    bank = []
+    for i in range(48):
+        dt = np.float32 if i % 2 else np.float64
+        src = src32 if dt == np.float32 else src64
+        cnt = max(1, int(np.exp(rng.uniform(lo, hi))) // np.dtype(dt).itemsize)
+        eb = None if i % 2 == 0 else float(10 ** rng.uniform(-6, -2))
+        bank.append((api.compress(src[:cnt], eb), np.dtype(dt), eb, cnt))
+
+    def make(n, rate):
+        reqs, t = [], 0.0
+        for k in range(n):
+            t += rng.exponential(1.0 / rate) if rate else 0.0
+            if rng.random() < 0.6:
+                dt = np.float32 if rng.random() < 0.5 else np.float64
+                src = src32 if dt == np.float32 else src64
+                cnt = max(1, int(np.exp(rng.uniform(lo, hi))) // np.dtype(dt).itemsize)
+                per16 = 16 // np.dtype(dt).itemsize  # request buffers start 16-byte aligned
+                off = int(rng.integers(0, (src.numel() - cnt) // per16)) * per16
+                eb = None if rng.random() < 0.5 else float(10 ** rng.uniform(-6, -2))
+                reqs.append(Request("compress", src[off:off + cnt], np.dtype(dt), eb, arrival=t, rid=k))
+            else:
+                st_, dt, eb, cnt = bank[int(rng.integers(0, len(bank)))]
+                reqs.append(Request("decompress", st_, dt, eb, num_elements=cnt, arrival=t, rid=k))
+        return reqs
+
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(150 << 30, free - (8 << 30)))
+    srv = Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
+    # peak: everything queued at once
+    warm = make(min(2000, n_requests), 0.0)
+    peak = srv.serve(warm)["gbs"]
+    reqs = make(n_requests, 0.0)
+    mean_bytes = np.mean([r.raw_bytes for r in reqs])
+    rate = 0.7 * peak * 1e9 / mean_bytes
+    t = 0.0
+    for r in reqs:
+        t += rng.exponential(1.0 / rate)
+        r.arrival = t
+    sample = set(int(i) for i in rng.choice(len(reqs), max(1, len(reqs) // 100), replace=False))
+    stats = srv.serve(reqs, keep=lambda r: r.rid in sample)
+    exact = True
+    for r in reqs:
+        if r.rid in sample:
+            got = srv.result(r)
+            alone = api.compress(r.src, r.eb) if r.op == "compress" else api.decompress(r.src, r.dtype, r.eb).view(
+                torch.uint8)
+            exact = exact and torch.equal(got, alone)
+            srv.release(r)
+    srv.close()
+    stats.update({"target_load": 0.7, "peak_gbs": peak, "arrival_rate_per_s": round(rate, 1),
+                  "hbm_budget_bytes": budget, "sample_checked": len(sample), "sample_bit_exact": bool(exact),
+                  "workload": f"{n_requests} requests, Poisson at 70% of peak, 1 KB-256 MB log-uniform, "
+                              "60/40 compress/decompress, 50% lossy eb in [1e-6,1e-2]"})
+    return stats
+
+
 def config_dict(args):
     return {"workload": "c1 f64 turbulence field 256x384x384 (301,989,888 B), lossless + eb 1e-2/1e-4/1e-6, "
                         "compress+decompress per mode",
@@ -343,6 +415,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1000-array) comparison")
+    ap.add_argument("--serve-requests", type=int, default=100000,
+                    help="requests of the served workload leg (0 = skip; 100000 = the full workload)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -543,6 +617,9 @@ def main():
         del enc, dec, d_in, d_enc, hin, hout, hstream
         torch.cuda.empty_cache()
         line["batched"] = bench_batched(dev, world, args)
+    if args.serve_requests > 0:
+        torch.cuda.empty_cache()
+        line["served"] = bench_serve(dev, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
     if rank == 0:

@@ -386,7 +386,17 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
           // chunk (the padding is encoded too)
           const uint32_t* const gin = reinterpret_cast<const uint32_t*>(in);
           uint32_t* const sv = reinterpret_cast<uint32_t*>(stg);
-          for (int k = lane; k < CS / 4; k += 32) sv[k] = 4 * k < osize ? gin[k] : 0u;
+          constexpr int U = 16;  // independent loads in flight per lane
+          for (int k0 = 0; k0 < CS / 4; k0 += 32 * U) {
+            uint32_t v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int k = k0 + u * 32 + lane;
+              v[u] = 4 * k < osize ? gin[k] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) sv[k0 + u * 32 + lane] = v[u];
+          }
           __syncwarp();
           if (lane == 0) {
             issued &= ~(1u << s);

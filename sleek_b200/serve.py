@@ -108,6 +108,7 @@ class _Slot:
     plans: dict
     ws: dict
     sizes: torch.Tensor
+    sizes_host: torch.Tensor  # pinned; filled by an async copy on the slot's stream
     busy: bool = False
     event: Optional[torch.cuda.Event] = None
     reqs: List[Request] = field(default_factory=list)
@@ -131,7 +132,8 @@ class Server:
             ws = {op: torch.zeros(8 * (32 + max_batch_chunks + 2 * max_batch), dtype=torch.uint8, device=device)
                   for op in ("compress", "decompress")}
             self.slots.append(_Slot(torch.cuda.Stream(device=device), plans, ws,
-                                    torch.zeros(2 * max_batch, dtype=torch.int64, device=device)))
+                                    torch.zeros(2 * max_batch, dtype=torch.int64, device=device),
+                                    torch.zeros(2 * max_batch, dtype=torch.int64, pin_memory=True)))
         self.queue: List[Request] = []
         self.completed: List[Request] = []
         self.t0 = time.perf_counter()
@@ -193,6 +195,8 @@ class Server:
                 for i, r in enumerate(part):
                     r._slot_index = k + i
                 k += len(part)
+            # sizes come back with the batch, without a host wait on the device
+            slot.sizes_host[:k].copy_(slot.sizes[:k], non_blocking=True)
             slot.event = torch.cuda.Event()
             slot.event.record(slot.stream)
 
@@ -201,7 +205,7 @@ class Server:
         n = 0
         for slot in self.slots:
             if slot.busy and slot.event.query():
-                sizes = slot.sizes[: len(slot.reqs)].cpu().tolist() if slot.reqs else []
+                sizes = slot.sizes_host[: len(slot.reqs)].tolist() if slot.reqs else []
                 t = self.now()
                 for r in slot.reqs:
                     r.done = t
