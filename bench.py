@@ -592,6 +592,13 @@ def main():
     t_launch = sum(per) / len(MODES)
     achieved = alg_bytes / (t_launch * 1e-3) / 1e9
 
+    # DRAM traffic of the dominant kernel per launch, from the committed ncu summary
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"k_{dom}_c1_f64.md")
+    if os.path.exists(prof):
+        for ln_ in open(prof):
+            if ln_.startswith("traffic_bytes_per_launch"):
+                traffic = int(ln_.split(":")[1].split()[0])
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
@@ -606,7 +613,9 @@ def main():
             "decompress": round(len(MODES) * N / (t_dec * 1e-3) / 1e9 / memcpy_gbs, 3)},
         "roofline": {"bound": "hbm", "kernel": f"k_{dom}<u64> (mean over the 4 modes)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 3), "peak_kind": f"of {peak_kind}", "traffic": None},
+                     "frac": round(achieved / peak, 3), "peak_kind": f"of {peak_kind}", "traffic": traffic,
+                     "traffic_note": "ncu DRAM read+write of one lossless launch (profiles/); the L2 still holds "
+                                     "part of the written stream when the kernel ends"},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * len(MODES) * args.steps,
