@@ -235,20 +235,46 @@ __device__ __forceinline__ uint32_t quant(uint32_t val, const QParams& q)
   return enc ? enc - 1u : 0u;
 }
 
+// 64-bit quantize on 32-bit halves (same arithmetic as the 64-bit form: the
+// rounding add carries into the high word, the shift is a funnel shift).
 __device__ __forceinline__ uint64_t quant(uint64_t val, const QParams& q)
 {
-  const uint64_t a = val & 0x7fffffffffffffffull;
-  const int ve = static_cast<int>(a >> 52);
-  uint64_t enc = 0;
+  const uint32_t h = static_cast<uint32_t>(val >> 32);
+  const uint32_t l = static_cast<uint32_t>(val);
+  const uint32_t ah = h & 0x7fffffffu;
+  const int ve = static_cast<int>(ah >> 20);
+  uint32_t eh = 0, el = 0;
   if (ve >= q.thr_e) {
-    enc = a - q.offs;
+    const uint32_t oh = static_cast<uint32_t>(q.offs >> 32);
+    const uint32_t ol = static_cast<uint32_t>(q.offs);
+    el = l - ol;
+    eh = ah - oh - (l < ol ? 1u : 0u);
   } else if (ve >= q.eb_e) {
-    const int sh = q.thr_e - ve;
-    const uint64_t mant = ((val & 0x000fffffffffffffull) | 0x0010000000000000ull) + (1ull << (sh - 1));
-    enc = mant >> sh;
+    const int sh = q.thr_e - ve;  // 1 .. 53
+    uint32_t mh = (h & 0x000fffffu) | 0x00100000u;
+    uint32_t ml = l;
+    const int b = sh - 1;
+    if (b < 32) {
+      const uint32_t add = 1u << b;
+      ml += add;
+      mh += ml < add ? 1u : 0u;
+    } else {
+      mh += 1u << (b - 32);
+    }
+    if (sh < 32) {
+      el = __funnelshift_r(ml, mh, sh);
+      eh = mh >> sh;
+    } else {
+      el = mh >> (sh - 32);
+    }
   }
-  enc = (enc << 1) | ((~val) >> 63);
-  return enc ? enc - 1ull : 0ull;
+  uint32_t rh = __funnelshift_l(el, eh, 1);
+  uint32_t rl = (el << 1) | ((h >> 31) ^ 1u);
+  if (rh | rl) {
+    rh -= rl == 0u ? 1u : 0u;
+    rl -= 1u;
+  }
+  return (static_cast<uint64_t>(rh) << 32) | rl;
 }
 
 __device__ __forceinline__ uint32_t dequant(uint32_t enc, const QParams& q)
@@ -265,18 +291,35 @@ __device__ __forceinline__ uint32_t dequant(uint32_t enc, const QParams& q)
   return dec | (enc << 31);
 }
 
+// 64-bit dequantize on 32-bit halves.
 __device__ __forceinline__ uint64_t dequant(uint64_t enc, const QParams& q)
 {
-  if (enc == 0ull) return 0ull;
-  const uint64_t a = (enc + 1ull) >> 1;
-  uint64_t dec = 0;
-  if (a >= (1ull << 52)) {
-    dec = a + q.offs;
-  } else if (a > 0ull) {
-    const int sh = __clzll(a) - 11;
-    dec = ((a << sh) & 0x000fffffffffffffull) | (static_cast<uint64_t>(q.thr_e - sh) << 52);
+  const uint32_t eh = static_cast<uint32_t>(enc >> 32);
+  const uint32_t el = static_cast<uint32_t>(enc);
+  if ((eh | el) == 0u) return 0ull;
+  const uint32_t tl = el + 1u;                      // (enc + 1) >> 1, wrapping like the 64-bit form
+  const uint32_t th = eh + (tl == 0u ? 1u : 0u);
+  const uint32_t ah = th >> 1;
+  const uint32_t al = __funnelshift_r(tl, th, 1);
+  uint32_t dh = 0, dl = 0;
+  if (ah >= (1u << 20)) {                            // a >= 2^52: stored losslessly
+    const uint32_t oh = static_cast<uint32_t>(q.offs >> 32);
+    const uint32_t ol = static_cast<uint32_t>(q.offs);
+    dl = al + ol;
+    dh = ah + oh + (dl < ol ? 1u : 0u);
+  } else if ((ah | al) != 0u) {
+    const int lz = ah ? __clz(ah) : 32 + __clz(al);
+    const int sh = lz - 11;                          // normalise the leading 1 to bit 52
+    if (sh < 32) {
+      dh = __funnelshift_l(al, ah, sh);
+      dl = al << sh;
+    } else {
+      dh = al << (sh - 32);
+    }
+    dh = (dh & 0x000fffffu) | (static_cast<uint32_t>(q.thr_e - sh) << 20);
   }
-  return dec | (enc << 63);
+  dh |= el << 31;                                    // sign from the lowest bit
+  return (static_cast<uint64_t>(dh) << 32) | dl;
 }
 
 template <bool LOSSY, typename T>
