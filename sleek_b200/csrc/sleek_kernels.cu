@@ -23,6 +23,7 @@
 namespace sleek {
 
 constexpr int ENC_STAGES = 4;
+constexpr int ENC_LAG = ENC_STAGES - 2;  // chunks computed but not yet stored
 constexpr int ENC_CW = 8;                    // compute warps
 constexpr int ENC_NT = (ENC_CW + 2) * 32;    // + a producer warp and a scanner warp
 constexpr int ENC_MINB = 3;
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       const int s = seq % ENC_STAGES;
       // From seq 2 on, the copy for chunk seq is issued when the compute warps
       // start chunk seq - 1: one chunk of lookahead, and the stage's previous
-      // chunk (seq - 4) has been stored by then.
+      // chunk (seq - ENC_STAGES) has been stored by then.
       if (seq >= 2) {
         const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1);
         if (__any_sync(0xffffffffu, !ok)) {
@@ -428,20 +429,24 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       EncMeta& me = m.meta[s];
       const long long g = me.g;
       if (g == NO_CHUNK) break;
+      // Looking back only once the chunk is sized: by then its predecessors have
+      // mostly published, so the look-back rarely polls twice.
+      const long long c = me.c;
+      long long excl = 0;
+      unsigned err = 0;
       ok = mbar_wait_bounded(&m.sized[s], par);
       if (__any_sync(0xffffffffu, !ok)) {
         if (lane == 0) set_status(ws, ST_TIMEOUT, g);
         break;
       }
-      const long long c = me.c;
-      const int csize = me.csize;
-      long long excl = 0;
       if (c > 0) {
         excl = lookback(flags, g, me.seg, ws);
-        unsigned err = 0;
         if (excl < 0) err = ST_TIMEOUT;
         else if (excl > c * CS) err = ST_CAPACITY;
         if (err) excl = -1;
+      }
+      const int csize = me.csize;
+      if (c > 0) {
         if (lane == 0) {
           if (err) set_status(ws, err, g);
           // an impossible prefix is replaced by the largest legal one so that
@@ -478,19 +483,28 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       }
     };
 
+    auto placed_store = [&](int sq) -> bool {  // false: the offset never arrived
+      const bool ok = mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1);
+      if (cbar_or(!ok)) {
+        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+        return false;
+      }
+      store(sq);
+      return true;
+    };
+
     int seq = 0;
     bool failed = false;
     for (;; ++seq) {
       const int s = seq % ENC_STAGES;
-      bool ok = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
-      if (seq >= 2) ok = mbar_wait_bounded(&m.placed[(seq - 2) % ENC_STAGES], ((seq - 2) / ENC_STAGES) & 1) && ok;
+      const bool ok = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
       if (cbar_or(!ok)) {
         if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
         failed = true;
         break;
       }
       // start of chunk seq: the producer may copy chunk seq + 1 into the stage of
-      // seq - 3, whose store every compute warp has finished
+      // seq + 1 - ENC_STAGES, whose store every compute warp has finished
       if (seq >= 1 && tid == 0) mbar_arrive(&m.empty[(seq + 1) % ENC_STAGES]);
       EncMeta& me = m.meta[s];
       if (me.g == NO_CHUNK) break;
@@ -505,18 +519,19 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
           default: compute_chunk<3>(stg, me, m, flags, cw, lane, tid); break;
         }
       }
-      // ---- store the chunk of seq - 2 (its offset is known) ---------------------
-      if (seq >= 2) store(seq - 2);
+      // ---- store the chunk of seq - ENC_LAG once its offset is known -----------
+      // (waiting here rather than before the compute gives its look-back one
+      // more chunk of compute time to finish)
+      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) {
+        failed = true;
+        break;
+      }
       fence_proxy_async_smem();  // generic accesses of this iteration before later TMA writes
     }
     if (!failed) {
-      // drain: chunks seq - 2 (placed already observed) and seq - 1
-      if (seq >= 2) store(seq - 2);
-      if (seq >= 1) {
-        const bool ok = mbar_wait_bounded(&m.placed[(seq - 1) % ENC_STAGES], ((seq - 1) / ENC_STAGES) & 1);
-        if (!cbar_or(!ok)) store(seq - 1);
-        else if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
-      }
+      // drain: chunks seq - ENC_LAG .. seq - 1
+      for (int q = seq >= ENC_LAG ? seq - ENC_LAG : 0; q < seq; ++q)
+        if (!placed_store(q)) break;
     }
   }
 
