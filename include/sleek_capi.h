@@ -181,6 +181,18 @@ int sleek_decompress_batch(const sleek_batch_item* items, int n, void* d_workspa
  * `stream`).  *status receives SLEEK_OK or the first device-side error. */
 int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
 
+/* Value range of a device array, NaNs ignored: *h_min and *h_max (host memory)
+ * receive its smallest and largest value (NaN when the array has no non-NaN
+ * value or is empty).  One HBM-bound pass on `stream` (NULL = legacy default
+ * stream), then a wait for it; uses the library-owned workspace of `stream`.
+ * Replaces the host loop of the range-relative error bound in the reference's
+ * ARTIFACT drivers (computeNOAeb, lossy_compressors_gpu/sleek_single_compressor_lossy.cu:59-75,
+ * sleek_double_compressor_lossy.cu:59-75), whose eb is (max - min) * parameter.
+ * Where the input holds NaNs the reference's result depends on its OpenMP
+ * schedule; this one ignores them. */
+int sleek_minmax_f32(const float* d_input, long long num_elements, float* h_min, float* h_max, void* stream);
+int sleek_minmax_f64(const double* d_input, long long num_elements, double* h_min, double* h_max, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdio>
+#include <cstdlib>
 #include <cuda_runtime.h>
 
 #include "sleek_capi.h"
@@ -15,6 +16,19 @@ static const int SLEEK_TPB = 512;       // kept for source compatibility; the li
 #ifndef SLEEK_WS
 #define SLEEK_WS 32
 #endif
+
+// CheckCuda of the reference (include/sleek_common_gpu.h:68-76), which its command-line
+// drivers call after each phase: waits for the device and exits with the same
+// message when a CUDA error is pending.
+static inline void CheckCuda(const int line)
+{
+  cudaDeviceSynchronize();
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "CUDA error %d on line %d: %s\n\n", e, line, cudaGetErrorString(e));
+    exit(-1);
+  }
+}
 
 // Reports a host- or device-side status the way the reference reports CUDA errors
 // (to stderr), but returns it instead of exiting.

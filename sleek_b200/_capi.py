@@ -65,6 +65,8 @@ SIGNATURES = {
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "sleek_set_ctas_per_sm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "sleek_minmax_f32": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp]),
+    "sleek_minmax_f64": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), _vp]),
     "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "sleek_batch_plan_workspace_size": (_sz, [_vp]),
     "sleek_batch_plan_create_reusable": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

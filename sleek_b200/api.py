@@ -220,3 +220,29 @@ def decompress(encoded: torch.Tensor, dtype, eb: Optional[float] = None, stream=
                              encoded_bytes=encoded.numel())
     m = _raise_if_negative(size, "decompress")
     return out[: m // dt.itemsize]
+
+
+def value_range(x: torch.Tensor, stream=None) -> tuple:
+    """(min, max) of a float32/float64 CUDA tensor on the device, NaNs ignored
+    (NaN, NaN when it holds no other value)."""
+    x = x.contiguous().view(-1)
+    _check_device(x)
+    dt = _np_dtype(x)
+    if dt == np.float32:
+        lo, hi = C.c_float(), C.c_float()
+        check(_capi.lib().sleek_minmax_f32(x.data_ptr(), x.numel(), C.byref(lo), C.byref(hi), _stream_handle(stream)),
+              "sleek_minmax_f32")
+    else:
+        lo, hi = C.c_double(), C.c_double()
+        check(_capi.lib().sleek_minmax_f64(x.data_ptr(), x.numel(), C.byref(lo), C.byref(hi), _stream_handle(stream)),
+              "sleek_minmax_f64")
+    return lo.value, hi.value
+
+
+def range_relative_error_bound(x: torch.Tensor, parameter: float) -> float:
+    """The absolute error bound of the reference's range-relative drivers,
+    (max - min) * parameter, computed in the array's own precision."""
+    lo, hi = value_range(x)
+    if x.dtype == torch.float32:
+        return float(np.float32(np.float32(hi) - np.float32(lo)) * np.float32(parameter))
+    return float((hi - lo) * parameter)

@@ -66,5 +66,54 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
+CLI_DIR = os.path.join(PKG, "cli")
+BIN_DIR = os.path.join(PKG, "_bin")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+# (program name, SLEEK_DOUBLE, SLEEK_LOSSY, SLEEK_DECOMPRESS): the names the
+# reference's build scripts give its GPU drivers (compile_compressors_*.sh)
+DRIVERS = [
+    (f"sleek_{p}_{'decompressor' if x else 'compressor'}_{'lossy' if l else 'lossless'}", d, l, x)
+    for d, p in ((0, "single"), (1, "double")) for l in (0, 1) for x in (0, 1)
+]
+
+
+def cli_programs() -> list[str]:
+    """Paths of every command-line program: the range-relative, timed drivers in
+    ``_bin`` (as the reference's scripts run them), the plain drivers in
+    ``_bin/standalone``, and ``_bin/GPUmemcpy``."""
+    out = [os.path.join(BIN_DIR, n) for n, *_ in DRIVERS]
+    out += [os.path.join(BIN_DIR, "standalone", n) for n, *_ in DRIVERS]
+    return out + [os.path.join(BIN_DIR, "GPUmemcpy")]
+
+
+def build_cli(force: bool = False, verbose: bool = False) -> list[str]:
+    """Compiles the command-line programs (host C++ over the C ABI) against the
+    library; a program is rebuilt when its source, the header or the library is newer."""
+    lib = build()
+    hdr = os.path.join(ROOT, "include", "sleek_capi.h")
+    common = ["g++", "-O2", "-std=c++17", "-Wall", f"-I{CUDA_HOME}/include", f"-I{os.path.join(ROOT, 'include')}"]
+    jobs = []
+    for name, d, l, x in DRIVERS:
+        for sub, extra in (("", ["-DARTIFACT"]), ("standalone", [])):
+            out = os.path.join(BIN_DIR, sub, name)
+            jobs.append((out, os.path.join(CLI_DIR, "sleek_driver.cpp"),
+                         [f"-DSLEEK_DOUBLE={d}", f"-DSLEEK_LOSSY={l}", f"-DSLEEK_DECOMPRESS={x}", *extra]))
+    jobs.append((os.path.join(BIN_DIR, "GPUmemcpy"), os.path.join(CLI_DIR, "gpu_memcpy.cpp"), []))
+    for out, src, defs in jobs:
+        deps = [src, hdr, lib, __file__]
+        if not force and os.path.exists(out) and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in deps):
+            continue
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        rel = os.path.relpath(LIB_DIR, os.path.dirname(out))
+        cmd = [*common, *defs, src, "-o", out, f"-L{LIB_DIR}", "-lsleek_b200", f"-L{CUDA_HOME}/lib64", "-lcudart",
+               f"-Wl,-rpath,$ORIGIN/{rel}:{CUDA_HOME}/lib64"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    return [j[0] for j in jobs]
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv))
+    print(len(build_cli(force="--force" in sys.argv)), "command-line programs in", BIN_DIR)

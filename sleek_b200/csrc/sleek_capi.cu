@@ -186,6 +186,51 @@ sleek::QParams qp(int eb_e, int thr_e, unsigned long long offs)
 
 }  // namespace
 
+namespace {
+
+template <typename F, typename U>
+int minmax(const F* in, long long n, F* h_min, F* h_max, void* stream)
+{
+  if (!h_min || !h_max || n < 0 || (n > 0 && !in)) return SLEEK_ERR_INVALID_ARG;
+  if (reinterpret_cast<uintptr_t>(in) % sizeof(F)) return SLEEK_ERR_ALIGNMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int dev = 0;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  uint64_t* w = nullptr;
+  rc = prepare_workspace(st, nullptr, 0, 8 * 3, &w);  // the two keys and a clear status word
+  if (rc) return rc;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned long long keys[2] = {0ull, 0ull};
+  if (sleek::launch_minmax(static_cast<int>(sizeof(F)), in, n, reinterpret_cast<unsigned long long*>(w),
+                           sms > 0 ? sms : 1, st) != cudaSuccess ||
+      cudaMemcpyAsync(keys, w, sizeof(keys), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return SLEEK_ERR_CUDA;
+  }
+  constexpr U top = static_cast<U>(1) << (8 * sizeof(U) - 1);
+  // a key with the top bit set came from a non-negative value, otherwise from a negative one
+  auto value = [&](U k) {
+    const U bits = (k & top) ? static_cast<U>(k ^ top) : static_cast<U>(~k);
+    F f;
+    std::memcpy(&f, &bits, sizeof(F));
+    return f;
+  };
+  if (keys[1] == 0ull) {  // no value that is not NaN
+    const U nan = sizeof(U) == 4 ? static_cast<U>(0x7fc00000u) : static_cast<U>(0x7ff8000000000000ull);
+    std::memcpy(h_min, &nan, sizeof(F));
+    std::memcpy(h_max, &nan, sizeof(F));
+    return SLEEK_OK;
+  }
+  *h_min = value(static_cast<U>(~static_cast<U>(keys[0])));  // keys[0]: inverted key of the minimum
+  *h_max = value(static_cast<U>(keys[1]));                   // keys[1]: key of the maximum
+  return SLEEK_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* sleek_status_string(int s)
@@ -333,6 +378,16 @@ int sleek_set_ctas_per_sm(int decompress, int elem_bytes, int lossy, int ctas_pe
   std::lock_guard<std::mutex> lk(g_mu);
   g_dev[dev].override_[elem_bytes == 8][lossy != 0][decompress == 0] = ctas_per_sm;
   return SLEEK_OK;
+}
+
+int sleek_minmax_f32(const float* in, long long n, float* h_min, float* h_max, void* stream)
+{
+  return minmax<float, uint32_t>(in, n, h_min, h_max, stream);
+}
+
+int sleek_minmax_f64(const double* in, long long n, double* h_min, double* h_max, void* stream)
+{
+  return minmax<double, uint64_t>(in, n, h_min, h_max, stream);
 }
 
 int sleek_workspace_status(const void* ws, void* stream, int* status)

@@ -75,5 +75,8 @@ cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st
 int encode_batch_blocks_per_sm();
 cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st);
 int blocks_per_sm(int width, bool lossy, bool enc);
+// min / max keys of a device array into keys[0] (inverted minimum) and keys[1]
+// (maximum); keys must be zero before the launch
+cudaError_t launch_minmax(int width, const void* in, long long n, unsigned long long* keys, int sms, cudaStream_t st);
 
 }  // namespace sleek
