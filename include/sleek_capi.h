@@ -181,6 +181,41 @@ int sleek_decompress_batch(const sleek_batch_item* items, int n, void* d_workspa
  * `stream`).  *status receives SLEEK_OK or the first device-side error. */
 int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
 
+/* ---- stream validation (host) ----------------------------------------------
+ * Parses a stream in HOST memory (no device call) and checks every rule the
+ * device decoders enforce: the 8-byte header (original size non-negative and a
+ * multiple of elem_bytes), the size table and every payload inside stream_len,
+ * each csize in [1, chunk bytes] and at least 34 for a compressed chunk, every
+ * subchunk bit width <= 8 * elem_bytes, the widths adding up to the csize, and
+ * the trailer equal to the chunk's byte count.  A stream passes exactly when
+ * the device decoders, given the same stream_len, accept it.  Returns SLEEK_OK
+ * or SLEEK_ERR_CORRUPT_STREAM (info says where and why), SLEEK_ERR_INVALID_ARG
+ * for a null pointer or an element size other than 4 or 8.  The reference has
+ * no such tool; its decoders trap on a malformed chunk (sleek_common_gpu.h:753,1264)
+ * and read out of bounds on a malformed table. */
+#define SLEEK_STREAM_OK             0
+#define SLEEK_STREAM_SHORT_HEADER   1  /* fewer than 8 bytes */
+#define SLEEK_STREAM_BAD_SIZE       2  /* original size negative or not a multiple of elem_bytes */
+#define SLEEK_STREAM_SHORT_TABLE    3  /* the size table runs past stream_len */
+#define SLEEK_STREAM_BAD_CHUNK_SIZE 4  /* csize 0, above the chunk's bytes, or below 34 while compressed */
+#define SLEEK_STREAM_SHORT_PAYLOAD  5  /* a payload runs past stream_len */
+#define SLEEK_STREAM_BAD_WIDTH      6  /* a subchunk bit width above the element width */
+#define SLEEK_STREAM_SIZE_MISMATCH  7  /* the bit widths do not add up to the csize */
+#define SLEEK_STREAM_BAD_TRAILER    8  /* the trailer differs from the chunk's byte count */
+
+typedef struct sleek_stream_info {
+  long long insize;        /* original bytes (header), -1 if unreadable */
+  long long chunks;        /* chunks the header implies */
+  long long stream_bytes;  /* 8 + 2 * chunks + sum of the csizes seen (the whole stream when valid) */
+  long long raw_chunks;    /* chunks stored verbatim */
+  long long bad_chunk;     /* first malformed chunk, -1 for header / table problems or none */
+  int reason;              /* SLEEK_STREAM_* */
+  int pad_;
+} sleek_stream_info;
+
+int sleek_validate_stream(const unsigned char* h_stream, long long stream_len, int elem_bytes, sleek_stream_info* info);
+const char* sleek_stream_reason_string(int reason);
+
 /* Value range of a device array, NaNs ignored: *h_min and *h_max (host memory)
  * receive its smallest and largest value (NaN when the array has no non-NaN
  * value or is empty).  One HBM-bound pass on `stream` (NULL = legacy default

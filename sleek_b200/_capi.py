@@ -43,6 +43,11 @@ class BatchItem(C.Structure):
 
 # every symbol the header declares: name -> (restype, argtypes)
 _i64 = C.c_longlong
+class StreamInfo(C.Structure):
+    _fields_ = [("insize", C.c_longlong), ("chunks", C.c_longlong), ("stream_bytes", C.c_longlong),
+                ("raw_chunks", C.c_longlong), ("bad_chunk", C.c_longlong), ("reason", C.c_int), ("pad_", C.c_int)]
+
+
 _vp = C.c_void_p
 _sz = C.c_size_t
 SIGNATURES = {
@@ -65,6 +70,8 @@ SIGNATURES = {
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "sleek_set_ctas_per_sm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "sleek_validate_stream": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
+    "sleek_stream_reason_string": (C.c_char_p, [C.c_int]),
     "sleek_minmax_f32": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp]),
     "sleek_minmax_f64": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), _vp]),
     "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

@@ -246,3 +246,26 @@ def range_relative_error_bound(x: torch.Tensor, parameter: float) -> float:
     if x.dtype == torch.float32:
         return float(np.float32(np.float32(hi) - np.float32(lo)) * np.float32(parameter))
     return float((hi - lo) * parameter)
+
+
+def validate_stream(stream, dtype) -> dict:
+    """Checks a stream held in host memory (bytes, bytearray, numpy or CPU
+    tensor) against every rule the device decoders enforce, without a device
+    call.  Returns ``{"valid", "reason", "reason_text", "bad_chunk", "insize",
+    "chunks", "stream_bytes", "raw_chunks"}``."""
+    if isinstance(stream, torch.Tensor):
+        if stream.is_cuda:
+            raise TypeError("validate_stream reads host memory")
+        stream = stream.contiguous().numpy()
+    buf = np.frombuffer(bytes(stream), dtype=np.uint8) if not isinstance(stream, np.ndarray) else \
+        np.ascontiguousarray(stream).view(np.uint8).reshape(-1)
+    info = _capi.StreamInfo()
+    L = _capi.lib()
+    rc = L.sleek_validate_stream(buf.ctypes.data if buf.size else None, buf.size, np.dtype(dtype).itemsize,
+                                 C.byref(info))
+    if rc not in (0, _capi.SLEEK_ERR_CORRUPT_STREAM):
+        check(rc, "sleek_validate_stream")
+    return {"valid": rc == 0, "reason": info.reason,
+            "reason_text": L.sleek_stream_reason_string(info.reason).decode(),
+            "bad_chunk": info.bad_chunk, "insize": info.insize, "chunks": info.chunks,
+            "stream_bytes": info.stream_bytes, "raw_chunks": info.raw_chunks}

@@ -81,10 +81,10 @@ DRIVERS = [
 def cli_programs() -> list[str]:
     """Paths of every command-line program: the range-relative, timed drivers in
     ``_bin`` (as the reference's scripts run them), the plain drivers in
-    ``_bin/standalone``, and ``_bin/GPUmemcpy``."""
+    ``_bin/standalone``, ``_bin/GPUmemcpy`` and ``_bin/sleek_validate``."""
     out = [os.path.join(BIN_DIR, n) for n, *_ in DRIVERS]
     out += [os.path.join(BIN_DIR, "standalone", n) for n, *_ in DRIVERS]
-    return out + [os.path.join(BIN_DIR, "GPUmemcpy")]
+    return out + [os.path.join(BIN_DIR, "GPUmemcpy"), os.path.join(BIN_DIR, "sleek_validate")]
 
 
 def build_cli(force: bool = False, verbose: bool = False) -> list[str]:
@@ -100,6 +100,7 @@ def build_cli(force: bool = False, verbose: bool = False) -> list[str]:
             jobs.append((out, os.path.join(CLI_DIR, "sleek_driver.cpp"),
                          [f"-DSLEEK_DOUBLE={d}", f"-DSLEEK_LOSSY={l}", f"-DSLEEK_DECOMPRESS={x}", *extra]))
     jobs.append((os.path.join(BIN_DIR, "GPUmemcpy"), os.path.join(CLI_DIR, "gpu_memcpy.cpp"), []))
+    jobs.append((os.path.join(BIN_DIR, "sleek_validate"), os.path.join(CLI_DIR, "sleek_validate.cpp"), []))
     for out, src, defs in jobs:
         deps = [src, hdr, lib, __file__]
         if not force and os.path.exists(out) and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in deps):

@@ -379,9 +379,14 @@ int main(int argc, char* argv[])
     fprintf(stderr, "ERROR: cannot read a stream header from %s\n\n", argv[1]);
     return -1;
   }
-  long long pre_size = 0;
-  std::memcpy(&pre_size, encoded, sizeof(pre_size));
-  if (pre_size < 0 || pre_size % static_cast<long long>(sizeof(F)) != 0) return fail("stream header", SLEEK_ERR_CORRUPT_STREAM);
+  // pre-flight: the whole stream is checked on the host before any device work
+  sleek_stream_info info;
+  if (sleek_validate_stream(encoded, insize, static_cast<int>(sizeof(F)), &info) != SLEEK_OK) {
+    fprintf(stderr, "ERROR: %s: %s (chunk %lld)\n\n", sleek_status_string(SLEEK_ERR_CORRUPT_STREAM),
+            sleek_stream_reason_string(info.reason), info.bad_chunk);
+    return -1;
+  }
+  const long long pre_size = info.insize;
   printf("encoded size: %lld bytes\n", insize);
 
   byte* decoded = nullptr;
