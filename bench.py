@@ -394,6 +394,48 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     return stats
 
 
+def bench_transfer(x, modes=(None, 1e-2, 1e-4), repeats=3):
+    """Compressed device->host and host->device copies of the field against plain
+    pinned cudaMemcpy of its N bytes: GB/s of uncompressed bytes, wall clock around
+    the synchronous calls (median of `repeats` after one warm-up); the assembled
+    host stream must equal the device stream byte for byte."""
+    from sleek_b200 import api
+
+    N = x.numel() * x.element_size()
+    hraw = torch.empty(N, dtype=torch.uint8, pin_memory=True)
+    hstream = torch.empty(api.sleek_upper_bound_size(N), dtype=torch.uint8, pin_memory=True)
+    back = torch.empty_like(x)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return sorted(ts)[len(ts) // 2]
+
+    xr = x.view(-1).view(torch.uint8)
+    out = {"workload": "c1 f64 field, 301,989,888 B, pinned host buffers, 32 MiB segments",
+           "plain_d2h_gbs": round(N / timed(lambda: hraw.copy_(xr)) / 1e9, 2),
+           "plain_h2d_gbs": round(N / timed(lambda: back.view(-1).view(torch.uint8).copy_(hraw)) / 1e9, 2)}
+    exact = True
+    for eb in modes:
+        h = api.compress_to_host(x, eb, out=hstream)
+        exact &= h.numpy().tobytes() == api.compress(x, eb).cpu().numpy().tobytes()
+        t_c = timed(lambda: api.compress_to_host(x, eb, out=hstream))
+        n = h.numel()
+        t_d = timed(lambda: api.decompress_from_host(hstream[:n], np.float64, eb, out=back))
+        if eb is None:
+            exact &= torch.equal(back.view(-1).view(torch.int64), x.view(-1).view(torch.int64))
+        out[str(eb)] = {"ratio": round(N / n, 3), "compress_to_host_gbs": round(N / t_c / 1e9, 2),
+                        "decompress_from_host_gbs": round(N / t_d / 1e9, 2)}
+    out["bit_exact"] = bool(exact)
+    return out
+
+
 def config_dict(args):
     return {"workload": "c1 f64 turbulence field 256x384x384 (301,989,888 B), lossless + eb 1e-2/1e-4/1e-6, "
                         "compress+decompress per mode",
@@ -415,6 +457,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1000-array) comparison")
+    ap.add_argument("--no-transfer", action="store_true", help="skip the compressed host<->device copy leg")
     ap.add_argument("--serve-requests", type=int, default=100000,
                     help="requests of the served workload leg (0 = skip; 100000 = the full workload)")
     args = ap.parse_args()
@@ -629,6 +672,8 @@ def main():
     if args.serve_requests > 0:
         torch.cuda.empty_cache()
         line["served"] = bench_serve(dev, args.serve_requests)
+    if not args.no_transfer:
+        line["transfer"] = bench_transfer(x)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
     if rank == 0:

@@ -181,6 +181,31 @@ int sleek_decompress_batch(const sleek_batch_item* items, int n, void* d_workspa
  * `stream`).  *status receives SLEEK_OK or the first device-side error. */
 int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
 
+/* ---- compressed transfers between device and host --------------------------
+ * The "compressing memory copy" use of the codec (the reference's README:1,4;
+ * its copy baseline is memcpy.cu:111-139): only the stream crosses PCIe.
+ *
+ * sleek_compress_to_host compresses a device array (elem_bytes 4 or 8, lossy 0/1,
+ * error_bound used when lossy) and leaves the complete stream -- byte for byte
+ * what sleek_compress_* writes -- in HOST memory h_encoded (h_capacity bytes;
+ * sleek_upper_bound_size always suffices), its length in *encoded_bytes.
+ * sleek_decompress_from_host checks a stream held in host memory with
+ * sleek_validate_stream, then decompresses it into device memory d_decoded
+ * (capacity_bytes), the byte count in *decoded_bytes.
+ *
+ * Both cut the array into segments of segment_bytes (0 = 32 MiB, rounded up to
+ * whole 16 KB chunks) so that the copy of one segment, on a library-owned copy
+ * stream, overlaps the codec work of the next on `stream` (NULL = legacy default
+ * stream).  Host buffers should be pinned (cudaMallocHost / cudaHostRegister) for
+ * the copies to overlap.  Both return when the result is complete; calls on one
+ * device are serialised.  Device staging: two segments' worth, kept per device. */
+int sleek_compress_to_host(const void* d_input, long long num_elements, int elem_bytes, int lossy, double error_bound,
+                           unsigned char* h_encoded, long long h_capacity, long long* encoded_bytes,
+                           long long segment_bytes, void* stream);
+int sleek_decompress_from_host(const unsigned char* h_encoded, long long encoded_bytes, int elem_bytes, int lossy,
+                               double error_bound, void* d_decoded, long long capacity_bytes, long long* decoded_bytes,
+                               long long segment_bytes, void* stream);
+
 /* ---- stream validation (host) ----------------------------------------------
  * Parses a stream in HOST memory (no device call) and checks every rule the
  * device decoders enforce: the 8-byte header (original size non-negative and a

@@ -70,6 +70,10 @@ SIGNATURES = {
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "sleek_set_ctas_per_sm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "sleek_compress_to_host": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_double, _vp, C.c_longlong,
+                                         C.POINTER(C.c_longlong), C.c_longlong, _vp]),
+    "sleek_decompress_from_host": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_double, _vp, C.c_longlong,
+                                             C.POINTER(C.c_longlong), C.c_longlong, _vp]),
     "sleek_validate_stream": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "sleek_stream_reason_string": (C.c_char_p, [C.c_int]),
     "sleek_minmax_f32": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp]),

@@ -269,3 +269,46 @@ def validate_stream(stream, dtype) -> dict:
             "reason_text": L.sleek_stream_reason_string(info.reason).decode(),
             "bad_chunk": info.bad_chunk, "insize": info.insize, "chunks": info.chunks,
             "stream_bytes": info.stream_bytes, "raw_chunks": info.raw_chunks}
+
+
+def compress_to_host(x: torch.Tensor, eb: Optional[float] = None, out: Optional[torch.Tensor] = None,
+                     segment_bytes: int = 0, stream=None) -> torch.Tensor:
+    """Compresses a float32/float64 CUDA tensor and returns its stream in pinned
+    host memory (a uint8 CPU tensor of the exact size): only the stream's bytes
+    cross PCIe, segment by segment, overlapped with the encoding of the next."""
+    x = x.contiguous().view(-1)
+    _check_device(x)
+    dt = _np_dtype(x)
+    cap = sleek_upper_bound_size(x.numel() * dt.itemsize)
+    if out is None:
+        out = torch.empty(max(cap, 16), dtype=torch.uint8, pin_memory=True)
+    if out.is_cuda or out.dtype != torch.uint8:
+        raise TypeError("out must be a uint8 CPU tensor")
+    n = C.c_longlong()
+    check(_capi.lib().sleek_compress_to_host(x.data_ptr(), x.numel(), dt.itemsize, int(eb is not None),
+                                             float(eb) if eb is not None else 0.0, out.data_ptr(), out.numel(),
+                                             C.byref(n), int(segment_bytes), _stream_handle(stream)),
+          "sleek_compress_to_host")
+    return out[: n.value]
+
+
+def decompress_from_host(encoded: torch.Tensor, dtype, eb: Optional[float] = None, out: Optional[torch.Tensor] = None,
+                         segment_bytes: int = 0, stream=None) -> torch.Tensor:
+    """Decompresses a stream held in host memory (a uint8 CPU tensor, ideally
+    pinned) into a CUDA tensor; the stream is validated on the host first and
+    only its bytes cross PCIe."""
+    if encoded.is_cuda or encoded.dtype != torch.uint8:
+        raise TypeError("encoded must be a uint8 CPU tensor")
+    encoded = encoded.contiguous()
+    dt = np.dtype(dtype)
+    tdt = torch.float32 if dt == np.float32 else torch.float64
+    n = int(encoded[:8].numpy().view(np.int64)[0]) if encoded.numel() >= 8 else -1
+    if out is None:
+        out = torch.empty(max(n // dt.itemsize, 1), dtype=tdt, device="cuda")
+    got = C.c_longlong()
+    check(_capi.lib().sleek_decompress_from_host(encoded.data_ptr(), encoded.numel(), dt.itemsize, int(eb is not None),
+                                                 float(eb) if eb is not None else 0.0, out.data_ptr(),
+                                                 out.numel() * out.element_size(), C.byref(got), int(segment_bytes),
+                                                 _stream_handle(stream)),
+          "sleek_decompress_from_host")
+    return out[: got.value // dt.itemsize]

@@ -186,6 +186,43 @@ sleek::QParams qp(int eb_e, int thr_e, unsigned long long offs)
 
 }  // namespace
 
+namespace sleek {
+
+// entry points for other host sources of the library (library-owned workspace of `stream`)
+int host_compress(int width, bool lossy, QParams q, const void* in, long long n, unsigned char* out,
+                  long long* outsize, void* stream)
+{
+  return do_compress(width, lossy, q, in, n, out, outsize, nullptr, 0, stream);
+}
+
+int host_decompress(int width, bool lossy, QParams q, const unsigned char* in, long long in_len, void* out,
+                    long long cap, long long* outsize, void* stream)
+{
+  return do_decompress(width, lossy, q, in, in_len, out, cap, outsize, nullptr, 0, stream);
+}
+
+int host_qparams(int width, bool lossy, double eb, QParams* q)
+{
+  q->eb_e = 0;
+  q->thr_e = 0;
+  q->offs = 0;
+  if (!lossy) return SLEEK_OK;
+  if (width == 4) {
+    sleek_eb_info_f32 e;
+    const int rc = sleek_error_bound_f32(static_cast<float>(eb), &e);
+    if (rc) return rc;
+    *q = qp(e.eb_e, e.thr_e, e.offs_e);
+  } else {
+    sleek_eb_info_f64 e;
+    const int rc = sleek_error_bound_f64(eb, &e);
+    if (rc) return rc;
+    *q = qp(e.eb_e, e.thr_e, e.offs_e);
+  }
+  return SLEEK_OK;
+}
+
+}  // namespace sleek
+
 namespace {
 
 template <typename F, typename U>

@@ -75,6 +75,14 @@ cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st
 int encode_batch_blocks_per_sm();
 cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st);
 int blocks_per_sm(int width, bool lossy, bool enc);
+// the single-buffer entry points for other host sources of the library (they use
+// the library-owned workspace of `stream`); host_qparams derives the quantizer
+// parameters of an error bound (SLEEK_ERR_ERROR_BOUND when it is too large)
+int host_compress(int width, bool lossy, QParams q, const void* in, long long n, unsigned char* out,
+                  long long* outsize, void* stream);
+int host_decompress(int width, bool lossy, QParams q, const unsigned char* in, long long in_len, void* out,
+                    long long cap, long long* outsize, void* stream);
+int host_qparams(int width, bool lossy, double eb, QParams* q);
 // min / max keys of a device array into keys[0] (inverted minimum) and keys[1]
 // (maximum); keys must be zero before the launch
 cudaError_t launch_minmax(int width, const void* in, long long n, unsigned long long* keys, int sms, cudaStream_t st);
