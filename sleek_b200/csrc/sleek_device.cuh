@@ -322,17 +322,81 @@ __device__ __forceinline__ uint64_t dequant(uint64_t enc, const QParams& q)
   return (static_cast<uint64_t>(dh) << 32) | dl;
 }
 
+// ----------------------------------------------------------------------------
+// The same quantize / dequantize with the rounding division done in floating
+// point (the integer forms above stay the definition; these are exact rewrites).
+//
+// Dequantize: for 0 < a < 2^m the integer form normalises a and sets the
+// exponent to thr_e - shift, which is the IEEE value a * 2^(thr_e - bias - m):
+// the int -> float conversion of a is exact (a < 2^m) and the power-of-two
+// product is exact and normal (its exponent field is at least thr_e - m >= 1).
+//
+// Quantize: for eb_e <= e < thr_e the integer form computes
+// floor((M + 2^(sh-1)) / 2^sh), M the significand with its implicit bit and
+// sh = thr_e - e.  With y = |v| * 2^(bias + m - thr_e) = M / 2^sh (exact: a
+// power-of-two scaling of a normal number with a normal result, y >= 1/2),
+// that is floor(y + 1/2).  y + 1/2 = N / 2^sh with N < 2^(m+2) is exact unless
+// N needs m + 2 bits and is odd; then rounding toward minus infinity yields
+// (N - 1) / 2^sh, and N odd with sh >= 1 means floor((N - 1) / 2^sh) =
+// floor(N / 2^sh).  So trunc(round_down(y + 1/2)) is exact.  Denormal values
+// (e = 0) are quantized only when eb_e = 0, where the integer form still adds
+// the implicit bit; that case keeps the integer form.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t quant_fp(uint32_t val, const QParams& q)
+{
+  if (q.eb_e == 0) return quant(val, q);
+  const uint32_t a = val & 0x7fffffffu;
+  const int ve = static_cast<int>(a >> 23);
+  const float inv_scale = __uint_as_float(static_cast<uint32_t>(277 - q.thr_e) << 23);  // 2^(150 - thr_e)
+  const uint32_t eq = __float2uint_rz(__fadd_rd(__fmul_rn(__uint_as_float(a), inv_scale), 0.5f));
+  uint32_t enc = ve >= q.thr_e ? a - static_cast<uint32_t>(q.offs) : (ve >= q.eb_e ? eq : 0u);
+  enc = (enc << 1) | ((~val) >> 31);
+  return enc ? enc - 1u : 0u;
+}
+
+__device__ __forceinline__ uint64_t quant_fp(uint64_t val, const QParams& q)
+{
+  if (q.eb_e == 0) return quant(val, q);
+  const uint64_t a = val & 0x7fffffffffffffffull;
+  const int ve = static_cast<int>(a >> 52);
+  const double inv_scale = __longlong_as_double(static_cast<long long>(2098 - q.thr_e) << 52);  // 2^(1075 - thr_e)
+  const uint64_t eq = __double2ull_rz(__dadd_rd(__dmul_rn(__longlong_as_double(static_cast<long long>(a)), inv_scale), 0.5));
+  uint64_t enc = ve >= q.thr_e ? a - q.offs : (ve >= q.eb_e ? eq : 0ull);
+  enc = (enc << 1) | ((~val) >> 63);
+  return enc ? enc - 1ull : 0ull;
+}
+
+__device__ __forceinline__ uint32_t dequant_fp(uint32_t enc, const QParams& q)
+{
+  if (enc == 0u) return 0u;
+  const uint32_t a = (enc + 1u) >> 1;
+  const float scale = __uint_as_float(static_cast<uint32_t>(q.thr_e - 23) << 23);  // 2^(thr_e - 150)
+  const uint32_t dec = a >= (1u << 23) ? a + static_cast<uint32_t>(q.offs)
+                                       : __float_as_uint(__fmul_rn(__uint2float_rn(a), scale));
+  return dec | (enc << 31);
+}
+
+__device__ __forceinline__ uint64_t dequant_fp(uint64_t enc, const QParams& q)
+{
+  if (enc == 0ull) return 0ull;
+  const uint64_t a = (enc + 1ull) >> 1;
+  const double scale = __longlong_as_double(static_cast<long long>(q.thr_e - 52) << 52);  // 2^(thr_e - 1075)
+  const uint64_t dec = a >= (1ull << 52) ? a + q.offs
+                                         : static_cast<uint64_t>(__double_as_longlong(__dmul_rn(__ull2double_rn(a), scale)));
+  return dec | (enc << 63);
+}
+
 template <bool LOSSY, typename T>
 __device__ __forceinline__ T encode_value(T v, const QParams& q)
 {
-  if constexpr (LOSSY) return quant(v, q);
+  if constexpr (LOSSY) return quant_fp(v, q);
   else return fwd(v);
 }
 
 template <bool LOSSY, typename T>
 __device__ __forceinline__ T decode_value(T v, const QParams& q)
 {
-  if constexpr (LOSSY) return dequant(v, q);
+  if constexpr (LOSSY) return dequant_fp(v, q);
   else return inv(v);
 }
 
