@@ -507,31 +507,39 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
 // ----------------------------------------------------------------------------
 // Shifted store: writes `len` bytes from 16-byte aligned shared memory `src`
 // to the arbitrary global byte address `dst`.  Whole aligned 16-byte granules
-// get one vector store each (a thread handles two neighbouring granules from
-// three aligned shared loads); the at most two granules shared with
-// neighbouring chunks are written byte by byte.  Called by all NT threads.
+// get one vector store each, funnel-shifted from two aligned shared loads; the
+// at most two granules shared with neighbouring chunks are written byte by
+// byte.  Called by all NT threads.
 // ----------------------------------------------------------------------------
 template <int WQ>
-__device__ __forceinline__ void shifted_pair(uint4* out, const uint4* s4, int j, int nfull_end, int bb8)
+__device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, int bb8)
 {
-  // output granules j and j+1 from source blocks j-1, j, j+1 (j >= 1)
-  const uint4 x = s4[j - 1];
-  const uint4 y = s4[j];
+  // output granule from source granules x = j - 1 and y = j
   const uint32_t w[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
   uint4 o;
   o.x = __funnelshift_r(w[WQ + 0], w[WQ + 1], bb8);
   o.y = __funnelshift_r(w[WQ + 1], w[WQ + 2], bb8);
   o.z = __funnelshift_r(w[WQ + 2], w[WQ + 3], bb8);
   o.w = __funnelshift_r(w[WQ + 3], w[WQ + 4], bb8);
-  out[j] = o;
-  if (j + 1 < nfull_end) {
-    const uint4 z = s4[j + 1];
-    const uint32_t u[8] = {y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w};
-    o.x = __funnelshift_r(u[WQ + 0], u[WQ + 1], bb8);
-    o.y = __funnelshift_r(u[WQ + 1], u[WQ + 2], bb8);
-    o.z = __funnelshift_r(u[WQ + 2], u[WQ + 3], bb8);
-    o.w = __funnelshift_r(u[WQ + 3], u[WQ + 4], bb8);
-    out[j + 1] = o;
+  return o;
+}
+
+// Granules jf .. jl-1, consecutive lanes on consecutive granules (so a warp's
+// loads hit every bank once and its stores fill whole sectors), two granules in
+// flight per thread.
+template <int WQ, int NT>
+__device__ __forceinline__ void shifted_run(uint4* out, const uint4* s4, int jf, int jl, int bb8)
+{
+  for (int j = jf + static_cast<int>(threadIdx.x); j < jl; j += 2 * NT) {
+    const bool two = j + NT < jl;
+    const uint4 x0 = s4[j - 1], y0 = s4[j];
+    uint4 x1 = x0, y1 = y0;
+    if (two) {
+      x1 = s4[j + NT - 1];
+      y1 = s4[j + NT];
+    }
+    out[j] = shifted_granule<WQ>(x0, y0, bb8);
+    if (two) out[j + NT] = shifted_granule<WQ>(x1, y1, bb8);
   }
 }
 
@@ -553,33 +561,25 @@ __device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, 
     const int bo = 16 - sft;
     const int bb8 = (bo & 3) * 8;
     switch (bo >> 2) {
-      case 0:
-        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<0>(out, s4, j, jl, bb8);
-        break;
-      case 1:
-        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<1>(out, s4, j, jl, bb8);
-        break;
-      case 2:
-        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<2>(out, s4, j, jl, bb8);
-        break;
-      default:
-        for (int j = jf + 2 * tid; j < jl; j += 2 * NT) shifted_pair<3>(out, s4, j, jl, bb8);
-        break;
+      case 0: shifted_run<0, NT>(out, s4, jf, jl, bb8); break;
+      case 1: shifted_run<1, NT>(out, s4, jf, jl, bb8); break;
+      case 2: shifted_run<2, NT>(out, s4, jf, jl, bb8); break;
+      default: shifted_run<3, NT>(out, s4, jf, jl, bb8); break;
     }
   }
-  // edge granules (shared with the neighbouring chunks): byte stores
-  if (tid < 2) {
+  // edge granules (shared with the neighbouring chunks): one byte per lane of
+  // the first warp, lanes 0-15 the first granule, lanes 16-31 the last
+  if (tid < 32) {
     int e = -1;
-    if (tid == 0 && sft != 0) e = 0;
-    if (tid == 1) {
+    if (tid < 16) {
+      if (sft != 0) e = 0;
+    } else {
       const int last = nunits - 1;
       if (last >= jl && !(last == 0 && sft != 0)) e = last;
     }
     if (e >= 0) {
-      const int r = 16 * e - sft;
-      const int b0 = r < 0 ? -r : 0;
-      const int b1 = (len - r) < 16 ? (len - r) : 16;
-      for (int b = b0; b < b1; b++) a0[16 * e + b] = src[r + b];
+      const int r = 16 * e - sft + (tid & 15);  // source byte of this lane
+      if (r >= 0 && r < len) a0[16 * e + (tid & 15)] = src[r];
     }
   }
 }
