@@ -189,9 +189,10 @@ int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
  * error_bound used when lossy) and leaves the complete stream -- byte for byte
  * what sleek_compress_* writes -- in HOST memory h_encoded (h_capacity bytes;
  * sleek_upper_bound_size always suffices), its length in *encoded_bytes.
- * sleek_decompress_from_host checks a stream held in host memory with
- * sleek_validate_stream, then decompresses it into device memory d_decoded
- * (capacity_bytes), the byte count in *decoded_bytes.
+ * sleek_decompress_from_host checks the header, size table and payload bounds
+ * of a stream held in host memory (the device decoder checks every chunk),
+ * then decompresses it into device memory d_decoded (capacity_bytes), the byte
+ * count in *decoded_bytes; a malformed stream is SLEEK_ERR_CORRUPT_STREAM either way.
  *
  * Both cut the array into segments of segment_bytes (0 = 32 MiB, rounded up to
  * whole 16 KB chunks) so that the copy of one segment, on a library-owned copy

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct sleek_stream_info;
+
 namespace sleek {
 
 constexpr int NT_MAX_WARPS = 32;
@@ -83,6 +85,10 @@ int host_compress(int width, bool lossy, QParams q, const void* in, long long n,
 int host_decompress(int width, bool lossy, QParams q, const unsigned char* in, long long in_len, void* out,
                     long long cap, long long* outsize, void* stream);
 int host_qparams(int width, bool lossy, double eb, QParams* q);
+// stream checks of sleek_validate_stream; with payloads = false only the header,
+// the size table and the payload bounds (what every copy of the stream depends
+// on), without reading the payloads themselves
+int validate_stream(const unsigned char* s, long long len, int elem_bytes, sleek_stream_info* info, bool payloads);
 // min / max keys of a device array into keys[0] (inverted minimum) and keys[1]
 // (maximum); keys must be zero before the launch
 cudaError_t launch_minmax(int width, const void* in, long long n, unsigned long long* keys, int sms, cudaStream_t st);

@@ -17,9 +17,10 @@
 //                      on `stream` into its place in the output
 //
 // so the PCIe transfer of one segment overlaps the codec work of the next.  The
-// host checks a received stream completely (sleek_validate_stream) before the
-// first copy.  Resources (copy stream, events, staging, pinned size slots) are
-// kept per device; calls on one device are serialised by a mutex.
+// host checks a received stream's header, size table and payload bounds before
+// the first copy; the device decoder checks every chunk.  Resources (copy
+// stream, events, staging, pinned size slots) are kept per device; calls on one
+// device are serialised by a mutex.
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -240,9 +241,12 @@ int sleek_decompress_from_host(const unsigned char* h_encoded, long long encoded
   if (rc) return rc;
   if (!h_encoded || !decoded_bytes || encoded_bytes < 0) return SLEEK_ERR_INVALID_ARG;
   if (reinterpret_cast<uintptr_t>(d_decoded) % elem_bytes) return SLEEK_ERR_ALIGNMENT;
-  // pre-flight: the whole stream, on the host, before any copy
+  // pre-flight on the host: header, size table and payload bounds, which every
+  // copy below relies on; each chunk's widths, size and trailer are checked by
+  // the device decoder (reading every chunk's header here would cost as much as
+  // a lossy stream's whole transfer)
   sleek_stream_info info;
-  rc = sleek_validate_stream(h_encoded, encoded_bytes, elem_bytes, &info);
+  rc = sleek::validate_stream(h_encoded, encoded_bytes, elem_bytes, &info, false);
   if (rc) return rc;
   const long long insize = info.insize;
   if (insize > capacity_bytes) return SLEEK_ERR_CAPACITY;

@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "../../include/sleek_capi.h"
+#include "sleek_launch.h"
 
 namespace {
 
@@ -39,6 +40,14 @@ const char* sleek_stream_reason_string(int reason)
 }
 
 int sleek_validate_stream(const unsigned char* s, long long len, int elem_bytes, sleek_stream_info* info)
+{
+  return sleek::validate_stream(s, len, elem_bytes, info, true);
+}
+
+}  // extern "C"
+
+int sleek::validate_stream(const unsigned char* s, long long len, int elem_bytes, sleek_stream_info* info,
+                           bool payloads)
 {
   if (!info || (!s && len > 0) || len < 0 || (elem_bytes != 4 && elem_bytes != 8)) return SLEEK_ERR_INVALID_ARG;
   std::memset(info, 0, sizeof(*info));
@@ -81,7 +90,7 @@ int sleek_validate_stream(const unsigned char* s, long long len, int elem_bytes,
     const unsigned char* p = s + off;
     if (cs == os) {
       info->raw_chunks++;
-    } else {
+    } else if (payloads) {
       long long bits = 0;
       for (int i = 0; i < 32; ++i) {
         if (p[i] > tb) {
@@ -107,4 +116,4 @@ int sleek_validate_stream(const unsigned char* s, long long len, int elem_bytes,
   return SLEEK_OK;
 }
 
-}  // extern "C"
+

@@ -2,8 +2,9 @@
 the stream assembled in host memory from independently encoded segments is
 byte-identical to the oracle's (and to a one-shot device compress) for one
 segment, many segments, ragged ends and empty arrays; decompressing from host
-memory reproduces the oracle's decode; malformed streams and short buffers are
-statuses raised before any device work."""
+memory reproduces the oracle's decode; malformed tables and short buffers are
+statuses raised before any device work, malformed chunks statuses from the
+device decoder."""
 import numpy as np
 import pytest
 import torch
@@ -60,6 +61,12 @@ def test_errors_before_device_work(cuda):
     s[8], s[9] = 0, 0  # first csize 0
     with pytest.raises(api.SleekError) as e:
         api.decompress_from_host(torch.frombuffer(s, dtype=torch.uint8), np.float64, 1e-3)
+    assert e.value.status == 5
+    # a chunk-level defect (a bit width above 64) is found by the device decoder
+    s = bytearray(O.encode(x, 1e-3))
+    s[8 + 2 * 10] = 65
+    with pytest.raises(api.SleekError) as e:
+        api.decompress_from_host(torch.frombuffer(s, dtype=torch.uint8), np.float64, 1e-3, segment_bytes=3 * CS)
     assert e.value.status == 5
     good = torch.frombuffer(bytearray(O.encode(x, 1e-3)), dtype=torch.uint8)
     small = torch.empty(10, dtype=torch.float64, device="cuda")
