@@ -52,7 +52,7 @@ struct EncMisc {
   uint64_t sized[ENC_STAGES];   // compressed size of the stage's chunk known
   uint64_t placed[ENC_STAGES];  // payload offset of the stage's chunk known
   EncMeta meta[ENC_STAGES];
-  int lnv[SC];
+  int lnv[2][SC];  // subchunk bit widths, by chunk parity (a fast warp may write the next chunk's)
 };
 
 constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
@@ -178,22 +178,27 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
 
 
 // Transform, size, publish and pack one chunk (compute warps).  KIND: bit 0 =
-// 64-bit values, bit 1 = lossy.
+// 64-bit values, bit 1 = lossy.  The barrier after phase A is the compute warps'
+// only CTA barrier per chunk and their point of agreement: every warp arrives
+// there, with `skip` (no chunk: the end, or a failed wait) and `fail` (this
+// thread's wait gave up); returns 2 if any thread failed, 1 at the end, 0 when
+// the chunk was processed.
 template <int KIND>
-__device__ __forceinline__ void compute_chunk(uint8_t* stg, EncMeta& me, EncMisc& m, uint64_t* flags, int cw,
-                                              int lane, int tid)
+__device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc& m, uint64_t* flags, int cw,
+                                             int lane, int tid, int par, bool skip, bool fail)
 {
   using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
   constexpr bool LOSSY = (KIND & 2) != 0;
   using V = VT<T>;
   constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane per subchunk
   constexpr int SPW = SC / ENC_CW;                      // subchunks per compute warp
-  const QParams q = me.q;
-  const int osize = me.osize;
+  int* const lnv = m.lnv[par];
 
   // ---- phase A: values into registers, transform / quantize, bit widths ------
   // (the stage always holds a full 16 KB chunk: partial chunks are zero padded)
   T vals[SPW][P];
+  if (!skip) {
+  const QParams q = me.q;
 #pragma unroll
   for (int u = 0; u < SPW; ++u) {
     const int i = cw + u * ENC_CW;
@@ -211,12 +216,15 @@ __device__ __forceinline__ void compute_chunk(uint8_t* stg, EncMeta& me, EncMisc
       orv |= vals[u][p];
     }
     const int w = warp_bit_width(orv);
-    if (lane == 0) m.lnv[i] = w;
+    if (lane == 0) lnv[i] = w;
   }
-  cbar();
+  }
+  if (cbar_or(fail)) return 2;
+  if (skip) return 1;
 
   // ---- widths scan (every warp, redundantly), size decision -----------------
-  const int ln_l = m.lnv[lane];
+  const int osize = me.osize;
+  const int ln_l = lnv[lane];
   const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
   int incl = wc;
 #pragma unroll
@@ -238,18 +246,20 @@ __device__ __forceinline__ void compute_chunk(uint8_t* stg, EncMeta& me, EncMisc
   // ---- pack this chunk from registers ----------------------------------------
   if (comp) {
     uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
+    int wbase[SPW], lnu[SPW];  // all offsets and widths first: the shuffles overlap
 #pragma unroll
     for (int u = 0; u < SPW; ++u) {
-      const int i = cw + u * ENC_CW;
-      const int wbase = __shfl_sync(0xffffffffu, incl - wc, i);
-      const int ln = __shfl_sync(0xffffffffu, ln_l, i);
-      pack_subchunk<T>(pw + wbase, ln, vals[u], lane);
+      wbase[u] = __shfl_sync(0xffffffffu, incl - wc, cw + u * ENC_CW);
+      lnu[u] = __shfl_sync(0xffffffffu, ln_l, cw + u * ENC_CW);
     }
+#pragma unroll
+    for (int u = 0; u < SPW; ++u) pack_subchunk<T>(pw + wbase[u], lnu[u], vals[u], lane);
     if (cw == 0) {
       stg[lane] = static_cast<uint8_t>(ln_l);
       if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
     }
   }
+  return 0;
 }
 
 // Chunk sources: one buffer (the plain entry points) or a table of buffers (the
@@ -328,7 +338,7 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
   if (tid == 0) {
     for (int s = 0; s < ENC_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
-      mbar_init(&m.empty[s], 1);
+      mbar_init(&m.empty[s], ENC_CW);  // one arrival per compute warp
       mbar_init(&m.sized[s], 1);
       mbar_init(&m.placed[s], 1);
     }
@@ -353,9 +363,9 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
     bool more = true;
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      // From seq 2 on, the copy for chunk seq is issued when the compute warps
-      // start chunk seq - 1: one chunk of lookahead, and the stage's previous
-      // chunk (seq - ENC_STAGES) has been stored by then.
+      // From seq 2 on, the copy for chunk seq is issued once every compute warp
+      // has finished chunk seq - 2 (one chunk of lookahead); the stage's previous
+      // chunk, seq - ENC_STAGES, was stored in that iteration.
       if (seq >= 2) {
         const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1);
         if (__any_sync(0xffffffffu, !ok)) {
@@ -483,50 +493,60 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       }
     };
 
-    auto placed_store = [&](int sq) -> bool {  // false: the offset never arrived
-      const bool ok = mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1);
-      if (cbar_or(!ok)) {
-        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+    // Each thread waits for the offset itself; a wait that gives up skips this
+    // thread's share of the store and is reported at the next barrier.
+    auto placed_store = [&](int sq) -> bool {
+      if (!mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1)) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
         return false;
       }
       store(sq);
       return true;
     };
 
+    // Warps pass each other freely between the barriers of compute_chunk: each
+    // waits for its stage and its offsets itself and frees a stage with its own
+    // arrival, and the pack data one warp stores were written by the others
+    // before an earlier barrier.
     int seq = 0;
     bool failed = false;
+    bool late = false;  // a wait of this thread gave up
     for (;; ++seq) {
       const int s = seq % ENC_STAGES;
-      const bool ok = mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1);
-      if (cbar_or(!ok)) {
-        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+      if (!mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1)) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
+        late = true;
+      }
+      EncMeta& me = m.meta[s];
+      // warp-uniform: phase A's warp collectives need every lane or none
+      const bool wlate = __any_sync(0xffffffffu, late);
+      const bool skip = wlate || me.g == NO_CHUNK;
+      uint8_t* const stg = stage0 + s * STAGE_BYTES;
+      int r;
+      if constexpr (KIND >= 0) {
+        r = compute_chunk<KIND>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate);
+      } else {
+        switch (skip ? 0 : me.kind) {
+          case 0: r = compute_chunk<0>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          case 1: r = compute_chunk<1>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          case 2: r = compute_chunk<2>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          default: r = compute_chunk<3>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+        }
+      }
+      if (r == 2) {
         failed = true;
         break;
       }
-      // start of chunk seq: the producer may copy chunk seq + 1 into the stage of
-      // seq + 1 - ENC_STAGES, whose store every compute warp has finished
-      if (seq >= 1 && tid == 0) mbar_arrive(&m.empty[(seq + 1) % ENC_STAGES]);
-      EncMeta& me = m.meta[s];
-      if (me.g == NO_CHUNK) break;
-      uint8_t* const stg = stage0 + s * STAGE_BYTES;
-      if constexpr (KIND >= 0) {
-        compute_chunk<KIND>(stg, me, m, flags, cw, lane, tid);
-      } else {
-        switch (me.kind) {
-          case 0: compute_chunk<0>(stg, me, m, flags, cw, lane, tid); break;
-          case 1: compute_chunk<1>(stg, me, m, flags, cw, lane, tid); break;
-          case 2: compute_chunk<2>(stg, me, m, flags, cw, lane, tid); break;
-          default: compute_chunk<3>(stg, me, m, flags, cw, lane, tid); break;
-        }
-      }
+      if (r == 1) break;
       // ---- store the chunk of seq - ENC_LAG once its offset is known -----------
       // (waiting here rather than before the compute gives its look-back one
       // more chunk of compute time to finish)
-      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) {
-        failed = true;
-        break;
-      }
-      fence_proxy_async_smem();  // generic accesses of this iteration before later TMA writes
+      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) late = true;
+      // this warp is done with the stage of seq - ENC_LAG, which the producer may
+      // now refill with chunk seq + 2 (generic accesses ordered before its TMA write)
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&m.empty[(seq + 2) % ENC_STAGES]);
     }
     if (!failed) {
       // drain: chunks seq - ENC_LAG .. seq - 1
