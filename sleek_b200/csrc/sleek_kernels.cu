@@ -607,9 +607,6 @@ struct DecMisc {
   long long vb;
   long long red[NT_MAX_WARPS];
   int bad[NT_MAX_WARPS];
-  int lnv[SC];
-  int bitbase[SC];
-  int ok;
   int abort;
 };
 
@@ -623,6 +620,63 @@ __device__ __forceinline__ uint64_t lds_u64_at_byte(const uint8_t* base, int byt
   const uint32_t lo = __funnelshift_r(w[wi], w[wi + 1], sh);
   const uint32_t hi = __funnelshift_r(w[wi + 1], w[wi + 2], sh);
   return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+// Decodes one staged chunk (payload at byte `sft` of `stg`, `cs` bytes, `osize`
+// bytes out) with the calling warp's share of the work and no CTA barrier: every
+// warp reads the 32 bit widths, scans and checks them itself (the same result in
+// every warp), then unpacks its subchunks cw, cw + NW, ... with consecutive lanes
+// on consecutive values, widths and bit offsets in registers.  Returns false for
+// a malformed chunk (bit width above the element width, widths not adding up to
+// cs, trailer not equal to osize); a raw chunk (cs == osize) is copied.
+template <typename T, bool LOSSY, int NW>
+__device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, int cs, int osize, T* o,
+                                                  const QParams& q, int cw, int lane)
+{
+  using V = VT<T>;
+  const int nv = osize / static_cast<int>(sizeof(T));
+  if (cs == osize) {
+    for (int e = cw * 32 + lane; e < nv; e += NW * 32) {
+      if constexpr (sizeof(T) == 4) o[e] = lds_u32_at_byte(stg, sft + 4 * e);
+      else o[e] = lds_u64_at_byte(stg, sft + 8 * e);
+    }
+    return true;
+  }
+  const int ln_l = stg[sft + lane];
+  const int bitsw = ln_l * V::VPS;
+  int incl = bitsw;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, k);
+    if (lane >= k) incl += t;
+  }
+  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+  bool ok = !__any_sync(0xffffffffu, ln_l > V::TB) && (34 + tot / 8 == cs);
+  if (ok) {
+    const int16_t tr = static_cast<int16_t>(stg[sft + cs - 2] | (stg[sft + cs - 1] << 8));
+    ok = tr == osize;
+  }
+  if (!ok) return false;
+  const int base_l = 8 * sft + 256 + incl - bitsw;  // first bit of subchunk `lane`
+  const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
+  for (int i = cw; i < SC; i += NW) {
+    const int ln = __shfl_sync(0xffffffffu, ln_l, i);
+    const int base = __shfl_sync(0xffffffffu, base_l, i);
+    const int k0 = i * V::VPS;
+    if (k0 >= nv) break;
+#pragma unroll
+    for (int j = lane; j < V::VPS; j += 32) {
+      if (k0 + j < nv) {
+        T e = 0;
+        if (ln) {
+          if constexpr (sizeof(T) == 4) e = extract_bits32(w, base + j * ln, ln);
+          else e = extract_bits64(w, base + j * ln, ln);
+        }
+        o[k0 + j] = decode_value<LOSSY>(e, q);
+      }
+    }
+  }
+  return true;
 }
 
 template <typename T, bool LOSSY, int NT, int MINB>
@@ -768,55 +822,9 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       uint8_t* const outc = a.out + c * CS;
       if (!d.ok) {
         if (tid == 0) set_status(ws, ST_CORRUPT, c);
-      } else if (d.cs == osize) {
-        // raw chunk: shifted copy from the staged bytes
-        T* const o = reinterpret_cast<T*>(outc);
-        const int nv = osize / static_cast<int>(sizeof(T));
-        for (int e = tid; e < nv; e += NT) {
-          if constexpr (sizeof(T) == 4) o[e] = lds_u32_at_byte(stg, d.sft + 4 * e);
-          else o[e] = lds_u64_at_byte(stg, d.sft + 8 * e);
-        }
-      } else {
-        if (warp == 0) {
-          const int ln = stg[d.sft + lane];
-          const int bitsw = ln * V::VPS;
-          int incl = bitsw;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-          }
-          const int tot = __shfl_sync(0xffffffffu, incl, 31);
-          m.lnv[lane] = ln;
-          m.bitbase[lane] = 8 * d.sft + 256 + incl - bitsw;
-          const bool bad_ln = __any_sync(0xffffffffu, ln > V::TB);
-          if (lane == 0) {
-            bool ok = !bad_ln && (34 + tot / 8 == d.cs);
-            if (ok) {
-              const int16_t tr = static_cast<int16_t>(stg[d.sft + d.cs - 2] | (stg[d.sft + d.cs - 1] << 8));
-              ok = tr == osize;
-            }
-            m.ok = ok;
-            if (!ok) set_status(ws, ST_CORRUPT, c);
-          }
-        }
-        __syncthreads();
-        if (m.ok) {
-          const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
-          T* const o = reinterpret_cast<T*>(outc);
-          const int nv = osize / static_cast<int>(sizeof(T));
-          for (int k = tid; k < nv; k += NT) {
-            const int i = k / V::VPS;
-            const int j = k - i * V::VPS;
-            const int ln = m.lnv[i];
-            T e = 0;
-            if (ln) {
-              if constexpr (sizeof(T) == 4) e = extract_bits32(w, m.bitbase[i] + j * ln, ln);
-              else e = extract_bits64(w, m.bitbase[i] + j * ln, ln);
-            }
-            o[k] = decode_value<LOSSY>(e, a.q);
-          }
-        }
+      } else if (!decode_chunk_warp<T, LOSSY, NW>(stg, d.sft, d.cs, osize, reinterpret_cast<T*>(outc), a.q,
+                                                    warp, lane)) {
+        if (tid == 0) set_status(ws, ST_CORRUPT, c);
       }
       fence_proxy_async_smem();
       __syncthreads();
@@ -861,9 +869,6 @@ struct DecBMisc {
   uint64_t full[DB_STAGES];
   uint64_t empty[DB_STAGES];
   DecBMeta meta[DB_STAGES];
-  int lnv[SC];
-  int bitbase[SC];
-  int ok;
 };
 
 constexpr int DB_SMEM = DB_STAGES * STAGE_BYTES + ((sizeof(DecBMisc) + 127) / 128) * 128 + 8 * (BATCH_MAX_JOBS + 1);
@@ -932,65 +937,6 @@ __global__ void __launch_bounds__(256) k_decode_prepass(const BatchDecArgs a)
   }
 }
 
-// Decode one staged chunk (compute warps).
-template <int KIND>
-__device__ __forceinline__ void decode_chunk(const uint8_t* stg, const DecBMeta& d, DecBMisc& m, uint64_t* ws,
-                                             int cw, int lane, int tid)
-{
-  using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
-  constexpr bool LOSSY = (KIND & 2) != 0;
-  using V = VT<T>;
-  constexpr int NT = DB_CW * 32;
-  const int osize = d.osize;
-  T* const o = reinterpret_cast<T*>(d.out);
-  const int nv = osize / static_cast<int>(sizeof(T));
-  if (d.cs == osize) {  // raw chunk: shifted copy from the staged bytes
-    for (int e = tid; e < nv; e += NT) {
-      if constexpr (sizeof(T) == 4) o[e] = lds_u32_at_byte(stg, d.sft + 4 * e);
-      else o[e] = lds_u64_at_byte(stg, d.sft + 8 * e);
-    }
-    return;
-  }
-  if (cw == 0) {
-    const int ln = stg[d.sft + lane];
-    const int bitsw = ln * V::VPS;
-    int incl = bitsw;
-#pragma unroll
-    for (int k = 1; k < 32; k <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, k);
-      if (lane >= k) incl += t;
-    }
-    const int tot = __shfl_sync(0xffffffffu, incl, 31);
-    m.lnv[lane] = ln;
-    m.bitbase[lane] = 8 * d.sft + 256 + incl - bitsw;
-    const bool bad_ln = __any_sync(0xffffffffu, ln > V::TB);
-    if (lane == 0) {
-      bool ok = !bad_ln && (34 + tot / 8 == d.cs);
-      if (ok) {
-        const int16_t tr = static_cast<int16_t>(stg[d.sft + d.cs - 2] | (stg[d.sft + d.cs - 1] << 8));
-        ok = tr == osize;
-      }
-      m.ok = ok;
-      if (!ok) set_status(ws, ST_CORRUPT, d.g);
-    }
-  }
-  cbar();
-  if (m.ok) {
-    const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
-    for (int k = tid; k < nv; k += NT) {
-      const int i = k / V::VPS;
-      const int jj = k - i * V::VPS;
-      const int ln = m.lnv[i];
-      T e = 0;
-      if (ln) {
-        if constexpr (sizeof(T) == 4) e = extract_bits32(w, m.bitbase[i] + jj * ln, ln);
-        else e = extract_bits64(w, m.bitbase[i] + jj * ln, ln);
-      }
-      o[k] = decode_value<LOSSY>(e, d.q);
-    }
-  }
-}
-
 __global__ void __launch_bounds__(DB_NT, DB_MINB) k_decode_batch(const BatchDecArgs a)
 {
   extern __shared__ __align__(128) uint8_t smem[];
@@ -1004,7 +950,7 @@ __global__ void __launch_bounds__(DB_NT, DB_MINB) k_decode_batch(const BatchDecA
   if (tid == 0) {
     for (int s = 0; s < DB_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
-      mbar_init(&m.empty[s], 1);
+      mbar_init(&m.empty[s], DB_CW);  // one arrival per compute warp
     }
     mbar_fence_init();
   }
@@ -1082,27 +1028,36 @@ __global__ void __launch_bounds__(DB_NT, DB_MINB) k_decode_batch(const BatchDecA
     }
   } else {
     // ===================== compute warps =====================
+    // No CTA barrier: each warp waits for a stage itself, decodes its share of the
+    // chunk and frees the stage with its own arrival.  A wait that gives up ends
+    // this warp's loop; the others and the producer end by their own bounded waits.
     for (int seq = 0;; ++seq) {
       const int s = seq % DB_STAGES;
-      const bool ok = mbar_wait_bounded(&m.full[s], (seq / DB_STAGES) & 1);
-      if (cbar_or(!ok)) {
-        if (tid == 0) set_status(ws, ST_TIMEOUT, -1);
+      if (__any_sync(0xffffffffu, !mbar_wait_bounded(&m.full[s], (seq / DB_STAGES) & 1))) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
         break;
       }
       const DecBMeta& d = m.meta[s];
       if (d.g == NO_CHUNK) break;
       if (d.state == 1) {
         const uint8_t* const stg = stage0 + s * STAGE_BYTES;
+        bool ok;
         switch (d.kind) {
-          case 0: decode_chunk<0>(stg, d, m, ws, warp, lane, tid); break;
-          case 1: decode_chunk<1>(stg, d, m, ws, warp, lane, tid); break;
-          case 2: decode_chunk<2>(stg, d, m, ws, warp, lane, tid); break;
-          default: decode_chunk<3>(stg, d, m, ws, warp, lane, tid); break;
+          case 0: ok = decode_chunk_warp<uint32_t, false, DB_CW>(stg, d.sft, d.cs, d.osize,
+                                                                 reinterpret_cast<uint32_t*>(d.out), d.q, warp, lane); break;
+          case 1: ok = decode_chunk_warp<uint64_t, false, DB_CW>(stg, d.sft, d.cs, d.osize,
+                                                                 reinterpret_cast<uint64_t*>(d.out), d.q, warp, lane); break;
+          case 2: ok = decode_chunk_warp<uint32_t, true, DB_CW>(stg, d.sft, d.cs, d.osize,
+                                                                reinterpret_cast<uint32_t*>(d.out), d.q, warp, lane); break;
+          default: ok = decode_chunk_warp<uint64_t, true, DB_CW>(stg, d.sft, d.cs, d.osize,
+                                                                 reinterpret_cast<uint64_t*>(d.out), d.q, warp, lane); break;
         }
+        if (!ok && warp == 0 && lane == 0) set_status(ws, ST_CORRUPT, d.g);
       }
+      // this warp is done with the stage (generic accesses ordered before the next TMA write)
       fence_proxy_async_smem();
-      cbar();
-      if (tid == 0) mbar_arrive(&m.empty[s]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&m.empty[s]);
     }
   }
 
