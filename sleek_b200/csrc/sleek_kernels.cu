@@ -600,9 +600,12 @@ struct DecChunk {
   int pad_;
 };
 
+constexpr int DEC_STAGES = 2;
+
 struct DecMisc {
-  uint64_t bar[2];
-  DecChunk info[2];
+  uint64_t full[DEC_STAGES];   // chunk bytes landed (TMA tx count)
+  uint64_t empty[DEC_STAGES];  // every compute warp is done with the stage's chunk
+  DecChunk info[DEC_STAGES];
   long long excl;
   long long vb;
   long long red[NT_MAX_WARPS];
@@ -610,7 +613,7 @@ struct DecMisc {
   int abort;
 };
 
-constexpr int DEC_SMEM = 2 * STAGE_BYTES + ((sizeof(DecMisc) + 127) / 128) * 128;
+constexpr int DEC_SMEM = DEC_STAGES * STAGE_BYTES + ((sizeof(DecMisc) + 127) / 128) * 128;
 
 __device__ __forceinline__ uint64_t lds_u64_at_byte(const uint8_t* base, int byte_off)
 {
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   constexpr int NW = NT / 32;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const stage0 = smem;
-  DecMisc& m = *reinterpret_cast<DecMisc*>(smem + 2 * STAGE_BYTES);
+  DecMisc& m = *reinterpret_cast<DecMisc*>(smem + DEC_STAGES * STAGE_BYTES);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -705,8 +708,10 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   const uint8_t* const data_in = a.in + 8 + 2 * chunks;
 
   if (tid == 0) {
-    mbar_init(&m.bar[0], 1);
-    mbar_init(&m.bar[1], 1);
+    for (int st = 0; st < DEC_STAGES; ++st) {
+      mbar_init(&m.full[st], 1);
+      mbar_init(&m.empty[st], NW);  // one arrival per warp
+    }
     mbar_fence_init();
     m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
     m.abort = 0;
@@ -794,26 +799,44 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
         d.sft = sft;
         d.ok = ok;
         if (ok) {
-          mbar_arrive_expect_tx(&m.bar[stg], nb);
-          tma_load_1d(stage0 + stg * STAGE_BYTES, src - sft, nb, &m.bar[stg]);
+          mbar_arrive_expect_tx(&m.full[stg], nb);
+          tma_load_1d(stage0 + stg * STAGE_BYTES, src - sft, nb, &m.full[stg]);
         } else {
-          mbar_arrive(&m.bar[stg]);
+          mbar_arrive(&m.full[stg]);
         }
       }
     };
 
-    if (warp == 0) issue(c0, 0);
+    // Warp 0 keeps DEC_STAGES - 1 chunks in flight: at chunk it it issues chunk
+    // it + DEC_STAGES - 1 into the stage of chunk it - 1, once every warp has
+    // released that stage.  No CTA barrier per chunk: each warp waits for its
+    // stages itself and releases them with its own arrival; a wait that gives up
+    // ends that warp's loop (the others end by their own bounded waits).
+    long long issued = c0;   // next chunk warp 0 issues
+    bool feeding = true;     // warp 0 still issues
+    auto issue_next = [&]() {  // warp 0, warp-uniform
+      const int jt = static_cast<int>(issued - c0);
+      const int st = jt % DEC_STAGES;
+      if (jt >= DEC_STAGES &&
+          __any_sync(0xffffffffu, !mbar_wait_bounded(&m.empty[st], ((jt - DEC_STAGES) / DEC_STAGES) & 1))) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, issued);
+        feeding = false;
+        return;
+      }
+      issue(issued, st);
+      ++issued;
+    };
+    if (warp == 0)
+      for (int k = 0; k < DEC_STAGES - 1 && issued < c1; ++k) issue_next();
     int it = 0;
-    for (long long c = c0; c < c1; ++c, ++it) {
-      const int s = it & 1;
+    long long c = c0;
+    for (; c < c1; ++c, ++it) {
+      const int s = it % DEC_STAGES;
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
-      if (warp == 0 && c + 1 < c1) issue(c + 1, s ^ 1);
+      if (warp == 0 && feeding && issued < c1) issue_next();
 
-      const bool arrived = mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
-      if (__syncthreads_or(!arrived)) {
-        if (tid == 0) set_status(ws, ST_TIMEOUT, c);
-        mbar_wait_bounded(&m.bar[s], (it >> 1) & 1);
-        if (c + 1 < c1) mbar_wait_bounded(&m.bar[s ^ 1], ((it + 1) >> 1) & 1);
+      if (__any_sync(0xffffffffu, !mbar_wait_bounded(&m.full[s], (it / DEC_STAGES) & 1))) {
+        if (lane == 0) set_status(ws, ST_TIMEOUT, c);
         break;
       }
 
@@ -826,8 +849,18 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
                                                     warp, lane)) {
         if (tid == 0) set_status(ws, ST_CORRUPT, c);
       }
+      // this warp is done with the stage (generic accesses ordered before the next TMA write)
       fence_proxy_async_smem();
-      __syncthreads();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&m.empty[s]);
+    }
+    // never leave with a bulk copy still landing in this CTA's shared memory:
+    // warp 0 waits for the chunks it issued but did not consume
+    if (warp == 0 && lane == 0) {
+      for (long long k = c; k < issued; ++k) {
+        const int jt = static_cast<int>(k - c0);
+        mbar_wait_bounded(&m.full[jt % DEC_STAGES], (jt / DEC_STAGES) & 1);
+      }
     }
   }
 
