@@ -242,6 +242,15 @@ typedef struct sleek_stream_info {
 int sleek_validate_stream(const unsigned char* h_stream, long long stream_len, int elem_bytes, sleek_stream_info* info);
 const char* sleek_stream_reason_string(int reason);
 
+/* Self-test of the device-side time limits (no counterpart in the reference, whose
+ * waits are unbounded): a one-warp kernel waits on an mbarrier that nothing arrives
+ * on and looks back over a predecessor flag that nothing publishes, each limited to
+ * limit_ns (0 < limit_ns <= 10 s), with the same wait helpers as the codec kernels.
+ * h_result[0] = 1 if the barrier wait gave up, h_result[1] = the look-back's result
+ * (-1 when it gave up), h_result[2] = nanoseconds both waits took.  Synchronous on
+ * the legacy default stream; the device stays usable. */
+int sleek_selftest_bounded_waits(long long limit_ns, long long* h_result);
+
 /* Value range of a device array, NaNs ignored: *h_min and *h_max (host memory)
  * receive its smallest and largest value (NaN when the array has no non-NaN
  * value or is empty).  One HBM-bound pass on `stream` (NULL = legacy default

@@ -76,6 +76,7 @@ SIGNATURES = {
                                              C.POINTER(C.c_longlong), C.c_longlong, _vp]),
     "sleek_validate_stream": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "sleek_stream_reason_string": (C.c_char_p, [C.c_int]),
+    "sleek_selftest_bounded_waits": (C.c_int, [C.c_longlong, C.POINTER(C.c_longlong)]),
     "sleek_minmax_f32": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp]),
     "sleek_minmax_f64": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), _vp]),
     "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

@@ -100,13 +100,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
   return ok != 0;
 }
 
-// Waits for the phase with the given parity; gives up after SPIN_TIMEOUT_NS.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+// Waits for the phase with the given parity; gives up after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  unsigned long long limit_ns = SPIN_TIMEOUT_NS)
 {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (globaltimer_ns() - t0 > SPIN_TIMEOUT_NS) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -444,11 +445,11 @@ __device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
 // (four independent loads per lane), sums the run of aggregates up to the
 // nearest inclusive prefix, and slides past runs of aggregates; it only waits
 // when the nearest unresolved flag is not published yet.  Returns the exclusive
-// prefix, or -1 when a wait exceeded SPIN_TIMEOUT_NS or another CTA already
+// prefix, or -1 when a wait exceeded `limit_ns` or another CTA already
 // reported an error.
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ long long lookback(const uint64_t* flags, long long idx, long long seg_begin,
-                                              const uint64_t* ws)
+                                              const uint64_t* ws, unsigned long long limit_ns = SPIN_TIMEOUT_NS)
 {
   constexpr int PER = 4;
   const int lane = threadIdx.x & 31;
@@ -493,7 +494,7 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
     if (++polls == 64) {
       t0 = globaltimer_ns();
     } else if (polls > 64 && (polls & 63) == 0) {
-      const bool late = globaltimer_ns() - t0 > SPIN_TIMEOUT_NS;
+      const bool late = globaltimer_ns() - t0 > limit_ns;
       const bool failed = ld_relaxed_u64(&ws[WS_STATUS]) != 0ull;
       if (__any_sync(0xffffffffu, late || failed)) return -1;
     }
