@@ -58,12 +58,7 @@ struct EncMisc {
 constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
 constexpr int ENC_BATCH_SMEM = ENC_SMEM + 8 * (BATCH_MAX_JOBS + 1);  // + the jobs' first chunk ids
 
-// barrier among the compute warps only (named barrier 1)
-__device__ __forceinline__ void cbar()
-{
-  asm volatile("bar.sync 1, %0;" ::"n"(ENC_CW * 32) : "memory");
-}
-
+// barrier among the compute warps only (named barrier 1), OR-reducing `pred`
 __device__ __forceinline__ bool cbar_or(bool pred)
 {
   uint32_t r;
@@ -610,7 +605,6 @@ struct DecMisc {
   long long vb;
   long long red[NT_MAX_WARPS];
   int bad[NT_MAX_WARPS];
-  int abort;
 };
 
 constexpr int DEC_SMEM = DEC_STAGES * STAGE_BYTES + ((sizeof(DecMisc) + 127) / 128) * 128;
@@ -714,7 +708,6 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
     }
     mbar_fence_init();
     m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
-    m.abort = 0;
     if (!hdr_ok) set_status(ws, ST_CORRUPT, -1);
     else if (!cap_ok) set_status(ws, ST_CAPACITY, -1);
   }
