@@ -394,6 +394,80 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     return stats
 
 
+def bench_configs(dev, reps=10):
+    """The other configurations of the measurement table on the same device path:
+    compress / decompress GB/s of uncompressed bytes and the compression ratio.
+    The C-ABI calls (workspace clear + kernel) are captured `reps` times in a CUDA
+    graph and replayed between CUDA events, so small inputs measure the device, not
+    the Python call overhead; each result is checked by a round trip (exact for
+    lossless, within the bound for lossy)."""
+    from sleek_b200 import _capi, api, workloads
+
+    L = _capi.lib()
+    cases = [("c0 f32 signal 2^24", lambda: workloads.c0_signal(device=dev), (None,)),
+             ("c2a f32 1800x3600", lambda: workloads.c2a_latlon(device=dev), (None, 1e-3)),
+             ("c2b f32 512^3", lambda: workloads.c2b_lognormal(device=dev), (None, 1e-3)),
+             ("c2c f32 2^28", lambda: workloads.c2c_particles(device=dev), (None, 1e-3))]
+    out = {}
+    side = torch.cuda.Stream(dev)
+    for name, make, ebs in cases:
+        x = make().contiguous().view(-1)
+        N = x.numel() * x.element_size()
+        row = {"bytes": N}
+        enc = torch.empty(api.sleek_upper_bound_size(N), dtype=torch.uint8, device=dev)
+        dec = torch.empty_like(x)
+        size = torch.zeros(2, dtype=torch.int64, device=dev)
+        wsz = max(L.sleek_compress_workspace_size(N), L.sleek_decompress_workspace_size())
+        ws = torch.zeros(wsz, dtype=torch.uint8, device=dev)
+        for eb in ebs:
+            sh = side.cuda_stream
+            if eb is None:
+                fc = lambda: L.sleek_compress_f32(x.data_ptr(), x.numel(), enc.data_ptr(), size.data_ptr(),
+                                                  ws.data_ptr(), wsz, sh)
+                fd = lambda: L.sleek_decompress_f32(enc.data_ptr(), enc.numel(), dec.data_ptr(), N,
+                                                    size[1:].data_ptr(), ws.data_ptr(), wsz, sh)
+            else:
+                e = api.sleek_error_bound(eb, np.float32).c_struct()
+                fc = lambda: L.sleek_compress_lossy_f32(e, x.data_ptr(), x.numel(), enc.data_ptr(),
+                                                        size.data_ptr(), ws.data_ptr(), wsz, sh)
+                fd = lambda: L.sleek_decompress_lossy_f32(e, enc.data_ptr(), enc.numel(), dec.data_ptr(), N,
+                                                          size[1:].data_ptr(), ws.data_ptr(), wsz, sh)
+            with torch.cuda.stream(side):
+                for _ in range(3):  # warm-up outside capture (grid sizes, attributes)
+                    _capi.check(fc())
+                    _capi.check(fd())
+            side.synchronize()
+            S = int(size[0].item())
+            assert int(size[1].item()) == N, name
+            if eb is None:
+                assert torch.equal(dec.view(torch.int32), x.view(torch.int32)), name
+            else:
+                fin = torch.isfinite(x)
+                assert bool(((dec[fin] - x[fin]).abs() <= eb).all()), name
+            res = {"ratio": round(N / S, 3)}
+            for lab, fn in (("compress_gbs", fc), ("decompress_gbs", fd)):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=side):
+                    for _ in range(reps):
+                        _capi.check(fn())
+                with torch.cuda.stream(side):  # replay() launches on the current stream
+                    g.replay()
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(side)
+                    g.replay()
+                    e1.record(side)
+                torch.cuda.synchronize()
+                res[lab] = round(N * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9, 1)
+                del g
+            row[str(eb)] = res
+        out[name] = row
+        del x, enc, dec, ws
+        torch.cuda.empty_cache()
+    out["timing"] = f"{reps} calls per CUDA graph replay, CUDA events"
+    return out
+
+
 def bench_transfer(x, modes=(None, 1e-2, 1e-4), repeats=3):
     """Compressed device->host and host->device copies of the field against plain
     pinned cudaMemcpy of its N bytes: GB/s of uncompressed bytes, wall clock around
@@ -458,6 +532,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1000-array) comparison")
     ap.add_argument("--no-transfer", action="store_true", help="skip the compressed host<->device copy leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the f32 configurations leg")
     ap.add_argument("--serve-requests", type=int, default=100000,
                     help="requests of the served workload leg (0 = skip; 100000 = the full workload)")
     args = ap.parse_args()
@@ -689,6 +764,8 @@ def main():
         line["served"] = bench_serve(dev, args.serve_requests)
     if not args.no_transfer:
         line["transfer"] = bench_transfer(x)
+    if not args.no_configs:
+        line["configs"] = bench_configs(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
     if rank == 0:
