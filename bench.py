@@ -166,6 +166,65 @@ def cpu_port_run(x: np.ndarray, repeats: int):
     return nbytes / t_total / 1e9
 
 
+def reference_gpu_kernels(x: torch.Tensor, reps: int = 5):
+    """The reference's own GPU codec (its headers compiled for sm_100a into
+    oracle/_ref) on the same field and modes: GB/s of uncompressed bytes through
+    its public API (which allocates and frees scratch per call) and with its kernels
+    launched on preallocated scratch; CUDA events on the legacy default stream it
+    uses.  Its streams must equal this project's.  None when it was not built."""
+    from oracle import oracle as O
+    from sleek_b200 import api
+
+    R = O.ref_gpu()
+    if R is None:
+        return None
+    blocks = R.ref_gpu_blocks()
+    N = x.numel() * 8
+    enc = torch.empty(api.sleek_upper_bound_size(N), dtype=torch.uint8, device=x.device)
+    dec = torch.empty_like(x)
+    size = torch.zeros(2, dtype=torch.int64, device=x.device)
+    carry = torch.zeros((N + 16383) // 16384 + 1, dtype=torch.int64, device=x.device)
+    dflt = torch.cuda.default_stream(x.device)
+
+    def timed(fn):
+        with torch.cuda.stream(dflt):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(dflt)
+            for _ in range(reps):
+                fn()
+            e1.record(dflt)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    out = {"kernels": "reference d_encode / d_decode built for sm_100a, grid %d x 512" % blocks, "modes": {}}
+    same = True
+    for eb in MODES:
+        lossy = int(eb is not None)
+        if eb is None:
+            api_c = lambda: R.ref_gpu_compress_f64(blocks, x.data_ptr(), x.numel(), enc.data_ptr(), size.data_ptr())
+            api_d = lambda: R.ref_gpu_decompress_f64(blocks, enc.data_ptr(), dec.data_ptr(), size[1:].data_ptr())
+        else:
+            api_c = lambda: R.ref_gpu_compress_lossy_f64(blocks, eb, x.data_ptr(), x.numel(), enc.data_ptr(),
+                                                         size.data_ptr())
+            api_d = lambda: R.ref_gpu_decompress_lossy_f64(blocks, eb, enc.data_ptr(), dec.data_ptr(),
+                                                           size[1:].data_ptr())
+        k_c = lambda: R.ref_gpu_encode_prealloc_f64(blocks, x.data_ptr(), x.numel(), enc.data_ptr(), size.data_ptr(),
+                                                    carry.data_ptr(), lossy, eb or 0.0)
+        k_d = lambda: R.ref_gpu_decode_prealloc_f64(blocks, enc.data_ptr(), dec.data_ptr(), size[1:].data_ptr(),
+                                                    carry.data_ptr(), lossy, eb or 0.0)
+        t_ac, t_kc = timed(api_c), timed(k_c)
+        S = int(size[0].item())
+        same &= enc[:S].cpu().numpy().tobytes() == api.compress(x, eb).cpu().numpy().tobytes()
+        t_ad, t_kd = timed(api_d), timed(k_d)
+        out["modes"][str(eb)] = {"compress_api_gbs": round(N / t_ac / 1e9, 1), "compress_kernel_gbs": round(N / t_kc / 1e9, 1),
+                                 "decompress_api_gbs": round(N / t_ad / 1e9, 1),
+                                 "decompress_kernel_gbs": round(N / t_kd / 1e9, 1)}
+    out["streams_identical_to_ours"] = bool(same)
+    return out
+
+
 def cpu_baseline(x_host: np.ndarray, max_seconds: float = 20.0):
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     cores = int(os.environ["OMP_NUM_THREADS"])
@@ -767,7 +826,10 @@ def main():
     if not args.no_configs:
         line["configs"] = bench_configs(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference's own implementations on this box: its CPU codec (the baseline)
+        # and, beside it, its GPU kernels built for sm_100a
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
+        line["reference_gpu"] = reference_gpu_kernels(x)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

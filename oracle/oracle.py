@@ -198,5 +198,9 @@ def ref_gpu():
             f = getattr(L, f"ref_gpu_decompress_{t}"); f.restype = None; f.argtypes = [_c.c_int, _vp, _vp, _vp]
             f = getattr(L, f"ref_gpu_compress_lossy_{t}"); f.restype = None; f.argtypes = [_c.c_int, ct, _vp, _i64, _vp, _vp]
             f = getattr(L, f"ref_gpu_decompress_lossy_{t}"); f.restype = None; f.argtypes = [_c.c_int, ct, _vp, _vp, _vp]
+            f = getattr(L, f"ref_gpu_encode_prealloc_{t}"); f.restype = None
+            f.argtypes = [_c.c_int, _vp, _i64, _vp, _vp, _vp, _c.c_int, _c.c_double]
+            f = getattr(L, f"ref_gpu_decode_prealloc_{t}"); f.restype = None
+            f.argtypes = [_c.c_int, _vp, _vp, _vp, _vp, _c.c_int, _c.c_double]
         _ref_gpu = L
     return _ref_gpu
