@@ -656,11 +656,13 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
   if (!ok) return false;
   const int base_l = 8 * sft + 256 + incl - bitsw;  // first bit of subchunk `lane`
   const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
-  for (int i = cw; i < SC; i += NW) {
+  static_assert(SC % NW == 0, "whole subchunks per warp");
+#pragma unroll
+  for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
+    const int i = cw + u * NW;
     const int ln = __shfl_sync(0xffffffffu, ln_l, i);
     const int base = __shfl_sync(0xffffffffu, base_l, i);
     const int k0 = i * V::VPS;
-    if (k0 >= nv) break;
 #pragma unroll
     for (int j = lane; j < V::VPS; j += 32) {
       if (k0 + j < nv) {
