@@ -221,13 +221,8 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
   const int osize = me.osize;
   const int ln_l = lnv[lane];
   const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
-  int incl = wc;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+  // totals by warp reductions (independent, no shuffle-scan chain)
+  const int wtot = __reduce_add_sync(0xffffffffu, wc);
   const int newsize = 34 + 4 * wtot;
   const bool comp = newsize < osize;
   const int csize = comp ? newsize : osize;
@@ -241,11 +236,12 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
   // ---- pack this chunk from registers ----------------------------------------
   if (comp) {
     uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
-    int wbase[SPW], lnu[SPW];  // all offsets and widths first: the shuffles overlap
+    int wbase[SPW], lnu[SPW];  // all offsets and widths first: the reductions overlap
 #pragma unroll
     for (int u = 0; u < SPW; ++u) {
-      wbase[u] = __shfl_sync(0xffffffffu, incl - wc, cw + u * ENC_CW);
-      lnu[u] = __shfl_sync(0xffffffffu, ln_l, cw + u * ENC_CW);
+      const int i = cw + u * ENC_CW;
+      wbase[u] = __reduce_add_sync(0xffffffffu, lane < i ? wc : 0);  // words of subchunks before i
+      lnu[u] = __shfl_sync(0xffffffffu, ln_l, i);
     }
 #pragma unroll
     for (int u = 0; u < SPW; ++u) pack_subchunk<T>(pw + wbase[u], lnu[u], vals[u], lane);
@@ -641,27 +637,20 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
   }
   const int ln_l = stg[sft + lane];
   const int bitsw = ln_l * V::VPS;
-  int incl = bitsw;
-#pragma unroll
-  for (int k = 1; k < 32; k <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, k);
-    if (lane >= k) incl += t;
-  }
-  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+  const int tot = __reduce_add_sync(0xffffffffu, bitsw);
   bool ok = !__any_sync(0xffffffffu, ln_l > V::TB) && (34 + tot / 8 == cs);
   if (ok) {
     const int16_t tr = static_cast<int16_t>(stg[sft + cs - 2] | (stg[sft + cs - 1] << 8));
     ok = tr == osize;
   }
   if (!ok) return false;
-  const int base_l = 8 * sft + 256 + incl - bitsw;  // first bit of subchunk `lane`
   const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
   static_assert(SC % NW == 0, "whole subchunks per warp");
 #pragma unroll
   for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
     const int i = cw + u * NW;
     const int ln = __shfl_sync(0xffffffffu, ln_l, i);
-    const int base = __shfl_sync(0xffffffffu, base_l, i);
+    const int base = 8 * sft + 256 + __reduce_add_sync(0xffffffffu, lane < i ? bitsw : 0);  // first bit of i
     const int k0 = i * V::VPS;
 #pragma unroll
     for (int j = lane; j < V::VPS; j += 32) {
