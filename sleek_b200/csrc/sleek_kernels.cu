@@ -1,22 +1,27 @@
-// sleek_kernels.cu -- sm_100a encode / decode kernels for one buffer.
+// sleek_kernels.cu -- sm_100a encode / decode kernels (one buffer, and batches).
 //
 // Encode (replaces d_encode, include/sleek_common_gpu.h:474-559, 989-1074 of the
-// reference): persistent CTAs take 16 KB chunks by atomic ticket, in order.  A
-// chunk arrives in shared memory by a 1-D TMA bulk copy issued one chunk ahead;
-// warps transform a subchunk each (value arithmetic restated from the reference)
-// and take the bit width from a warp max; warp 0 scans the widths, publishes the
-// chunk's compressed size and runs a bounded decoupled look-back while the other
-// warps pack the chunk in gather form (each thread assembles whole 64-bit words,
-// no shared atomics); finally all threads store the chunk at its byte offset with
-// 16-byte vector stores.  A chunk whose encoding is not smaller than its input is
-// stored raw straight from the staged copy (never re-read from HBM).
+// reference): persistent CTAs of 8 compute warps, a producer warp and a scanner
+// warp, 3 per SM.  The producer takes a chunk ticket (atomic, just in time) and
+// copies the 16 KB chunk into one of four shared-memory stages with a 1-D TMA bulk
+// copy, one chunk ahead.  Each compute warp loads 4 subchunks into registers,
+// transforms or quantizes them (value arithmetic restated from the reference) and
+// ORs them into bit widths; after the compute warps' one barrier per chunk every
+// warp derives the offsets it needs by warp reductions, thread 0 publishes the
+// chunk's size, and each warp packs its subchunks from registers (funnel-shifted
+// runs with one neighbour exchange; short runs by shared OR).  The scanner looks
+// back over the chunk flags and hands the payload offset to the compute warps,
+// which store the chunk two chunks later (16-byte vector stores, consecutive
+// lanes on consecutive granules).  A chunk whose encoding is not smaller than its
+// input is stored raw straight from the staged copy (never re-read from HBM).
 //
 // Decode (replaces d_decode, :688-768, 1199-1279): CTAs take contiguous chunk
 // ranges in ticket order, sum their ranges' compressed sizes, look back over the
 // preceding ranges once, then stream their chunks through a two-stage TMA
-// pipeline (each copy is the 16-byte aligned superset of the chunk's bytes) and
-// unpack with funnel shifts straight into coalesced global stores.  Malformed
-// streams set an error status instead of trapping.
+// pipeline (each copy is the 16-byte aligned superset of the chunk's bytes); every
+// warp checks each chunk itself and unpacks its own subchunks straight into
+// coalesced global stores, with no CTA barrier per chunk.  Malformed streams set
+// an error status instead of trapping; every wait is bounded in time.
 #include "sleek_device.cuh"
 #include "sleek_launch.h"
 
@@ -617,7 +622,7 @@ __device__ __forceinline__ uint64_t lds_u64_at_byte(const uint8_t* base, int byt
 
 // Decodes one staged chunk (payload at byte `sft` of `stg`, `cs` bytes, `osize`
 // bytes out) with the calling warp's share of the work and no CTA barrier: every
-// warp reads the 32 bit widths, scans and checks them itself (the same result in
+// warp reads the 32 bit widths, sums and checks them itself (the same result in
 // every warp), then unpacks its subchunks cw, cw + NW, ... with consecutive lanes
 // on consecutive values, widths and bit offsets in registers.  Returns false for
 // a malformed chunk (bit width above the element width, widths not adding up to
