@@ -199,7 +199,9 @@ int sleek_workspace_status(const void* d_workspace, void* stream, int* status);
  * stream, overlaps the codec work of the next on `stream` (NULL = legacy default
  * stream).  Host buffers should be pinned (cudaMallocHost / cudaHostRegister) for
  * the copies to overlap.  Both return when the result is complete; calls on one
- * device are serialised.  Device staging: two segments' worth, kept per device. */
+ * (device, stream) are serialised, calls on different streams run concurrently
+ * (e.g. a download thread and an upload thread keep both PCIe directions busy).
+ * Device staging: two segments' worth, kept per (device, stream). */
 int sleek_compress_to_host(const void* d_input, long long num_elements, int elem_bytes, int lossy, double error_bound,
                            unsigned char* h_encoded, long long h_capacity, long long* encoded_bytes,
                            long long segment_bytes, void* stream);

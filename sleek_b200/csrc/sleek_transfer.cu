@@ -19,12 +19,15 @@
 // so the PCIe transfer of one segment overlaps the codec work of the next.  The
 // host checks a received stream's header, size table and payload bounds before
 // the first copy; the device decoder checks every chunk.  Resources (copy
-// stream, events, staging, pinned size slots) are kept per device; calls on one
-// device are serialised by a mutex.
+// stream, events, staging, pinned size slots) are kept per (device, caller
+// stream); calls on one stream are serialised by a mutex, calls on different
+// streams run concurrently, so uploads and downloads can share the PCIe link
+// in both directions.
 #include <cstdint>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -59,12 +62,14 @@ struct Slots {
 };
 
 std::mutex g_map_mu;
-std::map<int, Slots*> g_slots;
+std::map<std::pair<int, void*>, Slots*> g_slots;
 
-Slots* slots_for(int dev)
+// resources of one (device, caller stream): calls on different streams of a
+// device run concurrently (each with its own copy stream and staging)
+Slots* slots_for(int dev, void* stream)
 {
   std::lock_guard<std::mutex> lk(g_map_mu);
-  Slots*& s = g_slots[dev];
+  Slots*& s = g_slots[{dev, stream}];
   if (!s) s = new Slots();  // kept until exit, like the library's workspaces
   return s;
 }
@@ -161,7 +166,7 @@ int sleek_compress_to_host(const void* d_input, long long num_elements, int elem
   const long long seg = segment_bytes_of(segment_bytes);
   const long long seg_chunks = seg / CS;
   const long long nseg = (chunks + seg_chunks - 1) / seg_chunks;
-  Slots* s = slots_for(dev);
+  Slots* s = slots_for(dev, stream);
   std::lock_guard<std::mutex> lk(s->mu);
   rc = prepare(s, seg, 2);
   if (rc) return rc;
@@ -263,7 +268,7 @@ int sleek_decompress_from_host(const unsigned char* h_encoded, long long encoded
   const long long seg = segment_bytes_of(segment_bytes);
   const long long seg_chunks = seg / CS;
   const long long nseg = (chunks + seg_chunks - 1) / seg_chunks;
-  Slots* s = slots_for(dev);
+  Slots* s = slots_for(dev, stream);
   std::lock_guard<std::mutex> lk(s->mu);
   rc = prepare(s, seg, nseg);
   if (rc) return rc;
