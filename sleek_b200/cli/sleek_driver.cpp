@@ -119,6 +119,15 @@ long long read_file(const char* name, byte** buf)
   return size;
 }
 
+// allocation or copy that must succeed; otherwise report and exit with 255
+void must(const cudaError_t e, const char* what)
+{
+  if (e != cudaSuccess) {
+    fprintf(stderr, "ERROR: %s failed: %s\n\n", what, cudaGetErrorString(e));
+    exit(-1);
+  }
+}
+
 bool write_file(const char* name, const byte* buf, long long size)
 {
   FILE* const f = fopen(name, "wb");
@@ -314,11 +323,11 @@ int main(int argc, char* argv[])
   F* d_input = nullptr;
   byte* d_encoded = nullptr;
   long long* d_encsize = nullptr;
-  cudaMallocHost(reinterpret_cast<void**>(&encoded), static_cast<size_t>(maxsize));
-  cudaMalloc(reinterpret_cast<void**>(&d_input), static_cast<size_t>(insize));
-  cudaMemcpy(d_input, input, static_cast<size_t>(insize), cudaMemcpyHostToDevice);
-  cudaMalloc(reinterpret_cast<void**>(&d_encoded), static_cast<size_t>(maxsize));
-  cudaMalloc(reinterpret_cast<void**>(&d_encsize), sizeof(long long));
+  must(cudaMallocHost(reinterpret_cast<void**>(&encoded), static_cast<size_t>(maxsize)), "host allocation");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_input), static_cast<size_t>(insize)), "device allocation");
+  must(cudaMemcpy(d_input, input, static_cast<size_t>(insize), cudaMemcpyHostToDevice), "copy to the device");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_encoded), static_cast<size_t>(maxsize)), "device allocation");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_encsize), sizeof(long long)), "device allocation");
   check_cuda(__LINE__);
 
 #if defined(ARTIFACT)
@@ -336,7 +345,7 @@ int main(int argc, char* argv[])
   const double runtime = timer.stop();
   if (rc) return fail("compress", rc);
   const long long encsize = result_size(d_encsize, "compress");
-  cudaMemcpy(encoded, d_encoded, static_cast<size_t>(encsize), cudaMemcpyDeviceToHost);
+  must(cudaMemcpy(encoded, d_encoded, static_cast<size_t>(encsize), cudaMemcpyDeviceToHost), "copy to the host");
   printf("encoded size: %lld bytes\n", encsize);
   check_cuda(__LINE__);
   const float CR = (100.0 * encsize) / insize;
@@ -352,7 +361,7 @@ int main(int argc, char* argv[])
 #endif
   if (int rc = run(d_input, num_elements, d_encoded, d_encsize, e32, e64)) return fail("compress", rc);
   const long long encsize = result_size(d_encsize, "compress");
-  cudaMemcpy(encoded, d_encoded, static_cast<size_t>(encsize), cudaMemcpyDeviceToHost);
+  must(cudaMemcpy(encoded, d_encoded, static_cast<size_t>(encsize), cudaMemcpyDeviceToHost), "copy to the host");
   printf("encoded size: %lld bytes\n", encsize);
   check_cuda(__LINE__);
   const float CR = (100.0 * encsize) / insize;
@@ -393,11 +402,13 @@ int main(int argc, char* argv[])
   byte* d_encoded = nullptr;
   F* d_decoded = nullptr;
   long long* d_decsize = nullptr;
-  cudaMallocHost(reinterpret_cast<void**>(&decoded), static_cast<size_t>(std::max(pre_size, 1ll)));
-  cudaMalloc(reinterpret_cast<void**>(&d_encoded), static_cast<size_t>(insize));
-  cudaMemcpy(d_encoded, encoded, static_cast<size_t>(insize), cudaMemcpyHostToDevice);
-  cudaMalloc(reinterpret_cast<void**>(&d_decoded), static_cast<size_t>(std::max(pre_size, 1ll)));
-  cudaMalloc(reinterpret_cast<void**>(&d_decsize), sizeof(long long));
+  must(cudaMallocHost(reinterpret_cast<void**>(&decoded), static_cast<size_t>(std::max(pre_size, 1ll))),
+       "host allocation");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_encoded), static_cast<size_t>(insize)), "device allocation");
+  must(cudaMemcpy(d_encoded, encoded, static_cast<size_t>(insize), cudaMemcpyHostToDevice), "copy to the device");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_decoded), static_cast<size_t>(std::max(pre_size, 1ll))),
+       "device allocation");
+  must(cudaMalloc(reinterpret_cast<void**>(&d_decsize), sizeof(long long)), "device allocation");
 
 #if defined(ARTIFACT)
 #if SLEEK_LOSSY
@@ -413,8 +424,8 @@ int main(int argc, char* argv[])
   }
   const F parameter = parse_value(argv[3]);
   F* d_orig = nullptr;
-  cudaMalloc(reinterpret_cast<void**>(&d_orig), static_cast<size_t>(insize_orig));
-  cudaMemcpy(d_orig, orig, static_cast<size_t>(insize_orig), cudaMemcpyHostToDevice);
+  must(cudaMalloc(reinterpret_cast<void**>(&d_orig), static_cast<size_t>(insize_orig)), "device allocation");
+  must(cudaMemcpy(d_orig, orig, static_cast<size_t>(insize_orig), cudaMemcpyHostToDevice), "copy to the device");
   const F eb = range_relative_bound(d_orig, insize_orig / static_cast<long long>(sizeof(F)), parameter);
   cudaFree(d_orig);
   if (int rc = error_bound_info(eb, &e32, &e64)) return fail("sleek_error_bound", rc);
@@ -428,7 +439,7 @@ int main(int argc, char* argv[])
   const double runtime = timer.stop();
   if (rc) return fail("decompress", rc);
   const long long decsize = result_size(d_decsize, "decompress");
-  cudaMemcpy(decoded, d_decoded, static_cast<size_t>(decsize), cudaMemcpyDeviceToHost);
+  must(cudaMemcpy(decoded, d_decoded, static_cast<size_t>(decsize), cudaMemcpyDeviceToHost), "copy to the host");
   printf("decoded size: %lld bytes\n", decsize);
   check_cuda(__LINE__);
 #if SLEEK_LOSSY
@@ -447,7 +458,7 @@ int main(int argc, char* argv[])
 #endif
   if (int rc = run(d_encoded, insize, d_decoded, pre_size, d_decsize, e32, e64)) return fail("decompress", rc);
   const long long decsize = result_size(d_decsize, "decompress");
-  cudaMemcpy(decoded, d_decoded, static_cast<size_t>(decsize), cudaMemcpyDeviceToHost);
+  must(cudaMemcpy(decoded, d_decoded, static_cast<size_t>(decsize), cudaMemcpyDeviceToHost), "copy to the host");
   printf("decoded size: %lld bytes\n", decsize);
   check_cuda(__LINE__);
   const float CR = (100.0 * insize) / decsize;
