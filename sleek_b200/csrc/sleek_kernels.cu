@@ -29,6 +29,9 @@ namespace sleek {
 
 constexpr int ENC_STAGES = 4;
 constexpr int ENC_LAG = ENC_STAGES - 2;  // chunks computed but not yet stored
+// the stage freed by storing chunk k - ENC_LAG (end of iteration k) takes chunk
+// k + ENC_AHEAD: the producer runs ENC_AHEAD - 1 chunks ahead of the compute warps
+constexpr int ENC_AHEAD = ENC_STAGES - ENC_LAG;
 constexpr int ENC_CW = 8;                    // compute warps
 constexpr int ENC_NT = (ENC_CW + 2) * 32;    // + a producer warp and a scanner warp
 constexpr int ENC_MINB = 3;
@@ -359,11 +362,11 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
     bool more = true;
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      // From seq 2 on, the copy for chunk seq is issued once every compute warp
-      // has finished chunk seq - 2 (one chunk of lookahead); the stage's previous
-      // chunk, seq - ENC_STAGES, was stored in that iteration.
-      if (seq >= 2) {
-        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - 2) / ENC_STAGES) & 1);
+      // From seq ENC_AHEAD on, the copy for chunk seq is issued once every compute
+      // warp has finished chunk seq - ENC_AHEAD, in which the stage's previous
+      // chunk, seq - ENC_STAGES, was stored.
+      if (seq >= ENC_AHEAD) {
+        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
         if (__any_sync(0xffffffffu, !ok)) {
           if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
           break;
@@ -539,10 +542,10 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       // more chunk of compute time to finish)
       if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) late = true;
       // this warp is done with the stage of seq - ENC_LAG, which the producer may
-      // now refill with chunk seq + 2 (generic accesses ordered before its TMA write)
+      // now refill with chunk seq + ENC_AHEAD (generic accesses ordered before its TMA write)
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&m.empty[(seq + 2) % ENC_STAGES]);
+      if (lane == 0) mbar_arrive(&m.empty[(seq + ENC_AHEAD) % ENC_STAGES]);
     }
     if (!failed) {
       // drain: chunks seq - ENC_LAG .. seq - 1
