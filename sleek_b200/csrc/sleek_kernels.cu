@@ -166,16 +166,21 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
     if (nfull > 2) d[2] = y2;
     if (nfull > 3) d[3] = y3;
   } else {
-    // short runs: several lanes share a word; clear the words, then OR in
-    const int words = (32 * P * ln) >> 5;
-    for (int q = lane; q < words; q += 32) pw[q] = 0u;
-    __syncwarp();
+    // short runs: several lanes share a word.  A run of R < 32 bits starts in
+    // every word, so the lane whose run starts first in a word stores it
+    // plainly (no clearing pass); the other lanes, and the spill of each run
+    // into the next word, OR in after that store.  Lane 31's run ends on a
+    // word boundary (32 R bits in all), so no spill leaves the packed area.
     uint32_t run = 0;
 #pragma unroll
     for (int k = 0; k < P; ++k) run |= static_cast<uint32_t>(v[k]) << (k * ln);
     const uint64_t sh = static_cast<uint64_t>(run) << s;
-    if (static_cast<uint32_t>(sh)) atomicOr(&pw[w0], static_cast<uint32_t>(sh));
-    if (static_cast<uint32_t>(sh >> 32)) atomicOr(&pw[w0 + 1], static_cast<uint32_t>(sh >> 32));
+    const uint32_t lo = static_cast<uint32_t>(sh), hi = static_cast<uint32_t>(sh >> 32);
+    const bool first = lane == 0 || (((lane - 1) * R) >> 5) != w0;
+    if (first) pw[w0] = lo;
+    __syncwarp();
+    if (!first && lo) atomicOr(&pw[w0], lo);
+    if (hi) atomicOr(&pw[w0 + 1], hi);
   }
 }
 
