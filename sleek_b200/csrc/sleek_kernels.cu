@@ -184,6 +184,122 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
   }
 }
 
+// The lane's bit run of P values of width ln as a 128-bit number x3:x2:x1:x0,
+// without branches, for 32 <= P*ln and ln < the value width.
+__device__ __forceinline__ void run_words(const uint32_t (&v)[4], int ln, uint32_t& x0, uint32_t& x1, uint32_t& x2,
+                                          uint32_t& x3)
+{
+  // pairs (v0 | v1 << ln) and (v2 | v3 << ln), each below 2^62; then the second
+  // pair shifted by 2 ln (16 .. 62) onto the first
+  const uint32_t a0 = v[0] | (v[1] << ln), a1 = __funnelshift_l(v[1], 0u, ln);
+  const uint32_t b0 = v[2] | (v[3] << ln), b1 = __funnelshift_l(v[3], 0u, ln);
+  const int k = 2 * ln;
+  const bool q = k >= 32;
+  const int r = k & 31;
+  const uint32_t t0 = b0 << r, t1 = __funnelshift_l(b0, b1, r), t2 = __funnelshift_l(b1, 0u, r);
+  x0 = a0 | (q ? 0u : t0);
+  x1 = a1 | (q ? t0 : t1);
+  x2 = q ? t1 : t2;
+  x3 = q ? t2 : 0u;
+}
+
+__device__ __forceinline__ void run_words(const uint64_t (&v)[2], int ln, uint32_t& x0, uint32_t& x1, uint32_t& x2,
+                                          uint32_t& x3)
+{
+  // v0 | v1 << ln with 16 <= ln <= 63 (below 32 both values fit in 32 bits)
+  const uint32_t a0 = static_cast<uint32_t>(v[0]), a1 = static_cast<uint32_t>(v[0] >> 32);
+  const uint32_t b0 = static_cast<uint32_t>(v[1]), b1 = static_cast<uint32_t>(v[1] >> 32);
+  const bool q = ln >= 32;
+  const int r = ln & 31;
+  const uint32_t t0 = b0 << r, t1 = __funnelshift_l(b0, b1, r), t2 = __funnelshift_l(b1, 0u, r);
+  x0 = a0 | (q ? 0u : t0);
+  x1 = a1 | (q ? t0 : t1);
+  x2 = q ? t1 : t2;
+  x3 = q ? t2 : 0u;
+}
+
+// Packs a warp's SPW subchunks (offsets wbase, widths lnu).  When every run is
+// short, or (32-bit values) every run is long (32 <= P*ln, ln below the value
+// width), the subchunks go through one straight-line sequence each, so their
+// shuffles, shifts and stores overlap; other widths take the per-subchunk path.
+// (For 64-bit values the branch-free long run costs more than the overlap saves:
+// measured -2 % on lossless f64, +3.5-6 % on f32.)
+constexpr int PACK_GROUP = 2;  // subchunks whose long runs are built and exchanged together
+
+template <typename T, int SPW>
+__device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[SPW], const int (&lnu)[SPW],
+                                               const T (&v)[SPW][16 / sizeof(T)], int lane)
+{
+  constexpr int P = 16 / static_cast<int>(sizeof(T));
+  constexpr int TB = 8 * static_cast<int>(sizeof(T));
+  bool all_long = sizeof(T) == 4, all_short = true;
+#pragma unroll
+  for (int u = 0; u < SPW; ++u) {
+    all_long &= P * lnu[u] >= 32 && lnu[u] < TB;
+    all_short &= P * lnu[u] < 32;
+  }
+  if (all_long) {
+#pragma unroll
+    for (int g = 0; g < SPW; g += PACK_GROUP) {
+    uint32_t y[SPW][5], tl[SPW], pv[SPW];
+    int nf[SPW];
+#pragma unroll
+    for (int u = g; u < g + PACK_GROUP; ++u) {
+      const int R = P * lnu[u];
+      const int s = (lane * R) & 31;
+      uint32_t x0, x1, x2, x3;
+      run_words(v[u], lnu[u], x0, x1, x2, x3);
+      y[u][0] = x0 << s;
+      y[u][1] = __funnelshift_l(x0, x1, s);
+      y[u][2] = __funnelshift_l(x1, x2, s);
+      y[u][3] = __funnelshift_l(x2, x3, s);
+      y[u][4] = __funnelshift_l(x3, 0u, s);
+      nf[u] = (s + R) >> 5;
+      tl[u] = nf[u] == 1 ? y[u][1] : (nf[u] == 2 ? y[u][2] : (nf[u] == 3 ? y[u][3] : y[u][4]));
+    }
+#pragma unroll
+    for (int u = g; u < g + PACK_GROUP; ++u) pv[u] = __shfl_up_sync(0xffffffffu, tl[u], 1);
+#pragma unroll
+    for (int u = g; u < g + PACK_GROUP; ++u) {
+      const int rs = lane * P * lnu[u];
+      uint32_t* const d = pw + wbase[u] + (rs >> 5);
+      d[0] = (rs & 31) ? (y[u][0] | pv[u]) : y[u][0];
+      if (nf[u] > 1) d[1] = y[u][1];
+      if (nf[u] > 2) d[2] = y[u][2];
+      if (nf[u] > 3) d[3] = y[u][3];
+    }
+    }
+  } else if (all_short) {
+    // see pack_subchunk: the first run in each word stores it, the rest OR in
+    uint32_t lo[SPW], hi[SPW];
+    int w[SPW];
+    bool first[SPW];
+#pragma unroll
+    for (int u = 0; u < SPW; ++u) {
+      const int ln = lnu[u];
+      const int R = P * ln;
+      uint32_t run = 0;
+#pragma unroll
+      for (int k = 0; k < P; ++k) run |= static_cast<uint32_t>(v[u][k]) << (k * ln);
+      const uint64_t sh = static_cast<uint64_t>(run) << ((lane * R) & 31);
+      lo[u] = static_cast<uint32_t>(sh);
+      hi[u] = static_cast<uint32_t>(sh >> 32);
+      w[u] = wbase[u] + ((lane * R) >> 5);
+      first[u] = ln != 0 && (lane == 0 || (((lane - 1) * R) >> 5) != ((lane * R) >> 5));
+      if (first[u]) pw[w[u]] = lo[u];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < SPW; ++u) {
+      if (!first[u] && lo[u]) atomicOr(&pw[w[u]], lo[u]);
+      if (hi[u]) atomicOr(&pw[w[u] + 1], hi[u]);
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < SPW; ++u) pack_subchunk<T>(pw + wbase[u], lnu[u], v[u], lane);
+  }
+}
+
 
 // Transform, size, publish and pack one chunk (compute warps).  KIND: bit 0 =
 // 64-bit values, bit 1 = lossy.  The barrier after phase A is the compute warps'
@@ -256,8 +372,7 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
       wbase[u] = __reduce_add_sync(0xffffffffu, lane < i ? wc : 0);  // words of subchunks before i
       lnu[u] = __shfl_sync(0xffffffffu, ln_l, i);
     }
-#pragma unroll
-    for (int u = 0; u < SPW; ++u) pack_subchunk<T>(pw + wbase[u], lnu[u], vals[u], lane);
+    pack_subchunks<T, SPW>(pw, wbase, lnu, vals, lane);
     if (cw == 0) {
       stg[lane] = static_cast<uint8_t>(ln_l);
       if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
