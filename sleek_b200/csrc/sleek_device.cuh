@@ -342,6 +342,10 @@ __device__ __forceinline__ uint64_t dequant(uint64_t enc, const QParams& q)
 // floor(N / 2^sh).  So trunc(round_down(y + 1/2)) is exact.  Denormal values
 // (e = 0) are quantized only when eb_e = 0, where the integer form still adds
 // the implicit bit; that case keeps the integer form.
+//
+// The sign step `e2 = (enc << 1) | !sign; e2 ? e2 - 1 : 0` is written as
+// `(enc << 1) - (enc ? sign : 0)`: for enc > 0 both are 2 enc - sign, and for
+// enc = 0 both are 0 (e2 is 1 - sign there).
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t quant_fp(uint32_t val, const QParams& q)
 {
@@ -351,8 +355,7 @@ __device__ __forceinline__ uint32_t quant_fp(uint32_t val, const QParams& q)
   const float inv_scale = __uint_as_float(static_cast<uint32_t>(277 - q.thr_e) << 23);  // 2^(150 - thr_e)
   const uint32_t eq = __float2uint_rz(__fadd_rd(__fmul_rn(__uint_as_float(a), inv_scale), 0.5f));
   uint32_t enc = ve >= q.thr_e ? a - static_cast<uint32_t>(q.offs) : (ve >= q.eb_e ? eq : 0u);
-  enc = (enc << 1) | ((~val) >> 31);
-  return enc ? enc - 1u : 0u;
+  return (enc << 1) - (enc ? (val >> 31) : 0u);
 }
 
 __device__ __forceinline__ uint64_t quant_fp(uint64_t val, const QParams& q)
@@ -363,8 +366,7 @@ __device__ __forceinline__ uint64_t quant_fp(uint64_t val, const QParams& q)
   const double inv_scale = __longlong_as_double(static_cast<long long>(2098 - q.thr_e) << 52);  // 2^(1075 - thr_e)
   const uint64_t eq = __double2ull_rz(__dadd_rd(__dmul_rn(__longlong_as_double(static_cast<long long>(a)), inv_scale), 0.5));
   uint64_t enc = ve >= q.thr_e ? a - q.offs : (ve >= q.eb_e ? eq : 0ull);
-  enc = (enc << 1) | ((~val) >> 63);
-  return enc ? enc - 1ull : 0ull;
+  return (enc << 1) - (enc ? (val >> 63) : 0ull);
 }
 
 __device__ __forceinline__ uint32_t dequant_fp(uint32_t enc, const QParams& q)

@@ -774,23 +774,36 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
   if (!ok) return false;
   const uint32_t* const w = reinterpret_cast<const uint32_t*>(stg);
   static_assert(SC % NW == 0, "whole subchunks per warp");
+  // full chunks (all but a stream's last) are unpacked without the per-value
+  // bound test (f32 lossy decode +11 %); 64-bit chunks whose widths are all at
+  // most 32 (typical of lossy streams) extract each value from two words
+  // instead of three (f64 lossy decode +23 %)
+  auto unpack = [&](auto full, auto narrow) {
 #pragma unroll
-  for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
-    const int i = cw + u * NW;
-    const int ln = __shfl_sync(0xffffffffu, ln_l, i);
-    const int base = 8 * sft + 256 + __reduce_add_sync(0xffffffffu, lane < i ? bitsw : 0);  // first bit of i
-    const int k0 = i * V::VPS;
+    for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
+      const int i = cw + u * NW;
+      const int ln = __shfl_sync(0xffffffffu, ln_l, i);
+      const int base = 8 * sft + 256 + __reduce_add_sync(0xffffffffu, lane < i ? bitsw : 0);  // first bit of i
+      const int k0 = i * V::VPS;
 #pragma unroll
-    for (int j = lane; j < V::VPS; j += 32) {
-      if (k0 + j < nv) {
-        T e = 0;
-        if (ln) {
-          if constexpr (sizeof(T) == 4) e = extract_bits32(w, base + j * ln, ln);
-          else e = extract_bits64(w, base + j * ln, ln);
+      for (int j = lane; j < V::VPS; j += 32) {
+        if (decltype(full)::value || k0 + j < nv) {
+          T e = 0;
+          if (ln) {
+            if constexpr (sizeof(T) == 4 || decltype(narrow)::value) e = extract_bits32(w, base + j * ln, ln);
+            else e = extract_bits64(w, base + j * ln, ln);
+          }
+          o[k0 + j] = decode_value<LOSSY>(e, q);
         }
-        o[k0 + j] = decode_value<LOSSY>(e, q);
       }
     }
+  };
+  if (sizeof(T) == 8 && __all_sync(0xffffffffu, ln_l <= 32)) {
+    if (osize == CS) unpack(std::true_type{}, std::true_type{});
+    else unpack(std::false_type{}, std::true_type{});
+  } else {
+    if (osize == CS) unpack(std::true_type{}, std::false_type{});
+    else unpack(std::false_type{}, std::false_type{});
   }
   return true;
 }
