@@ -343,6 +343,11 @@ __device__ __forceinline__ uint64_t dequant(uint64_t enc, const QParams& q)
 // (e = 0) are quantized only when eb_e = 0, where the integer form still adds
 // the implicit bit; that case keeps the integer form.
 //
+// Below eb_e the integer form gives 0, and so does eq without a test: e < eb_e
+// means |v| < 2^(eb_e - bias), so y < 2^(eb_e + m - thr_e) = 1/2 (thr_e =
+// eb_e + m + 1), y + 1/2 < 1 and its round-down truncates to 0 (a product that
+// underflows is rounded, but far below 1/2).
+//
 // The sign step `e2 = (enc << 1) | !sign; e2 ? e2 - 1 : 0` is written as
 // `(enc << 1) - (enc ? sign : 0)`: for enc > 0 both are 2 enc - sign, and for
 // enc = 0 both are 0 (e2 is 1 - sign there).
@@ -354,7 +359,7 @@ __device__ __forceinline__ uint32_t quant_fp(uint32_t val, const QParams& q)
   const int ve = static_cast<int>(a >> 23);
   const float inv_scale = __uint_as_float(static_cast<uint32_t>(277 - q.thr_e) << 23);  // 2^(150 - thr_e)
   const uint32_t eq = __float2uint_rz(__fadd_rd(__fmul_rn(__uint_as_float(a), inv_scale), 0.5f));
-  uint32_t enc = ve >= q.thr_e ? a - static_cast<uint32_t>(q.offs) : (ve >= q.eb_e ? eq : 0u);
+  const uint32_t enc = ve >= q.thr_e ? a - static_cast<uint32_t>(q.offs) : eq;
   return (enc << 1) - (enc ? (val >> 31) : 0u);
 }
 
@@ -365,7 +370,7 @@ __device__ __forceinline__ uint64_t quant_fp(uint64_t val, const QParams& q)
   const int ve = static_cast<int>(a >> 52);
   const double inv_scale = __longlong_as_double(static_cast<long long>(2098 - q.thr_e) << 52);  // 2^(1075 - thr_e)
   const uint64_t eq = __double2ull_rz(__dadd_rd(__dmul_rn(__longlong_as_double(static_cast<long long>(a)), inv_scale), 0.5));
-  uint64_t enc = ve >= q.thr_e ? a - q.offs : (ve >= q.eb_e ? eq : 0ull);
+  const uint64_t enc = ve >= q.thr_e ? a - q.offs : eq;
   return (enc << 1) - (enc ? (val >> 63) : 0ull);
 }
 
@@ -387,6 +392,18 @@ __device__ __forceinline__ uint64_t dequant_fp(uint64_t enc, const QParams& q)
   const uint64_t dec = a >= (1ull << 52) ? a + q.offs
                                          : static_cast<uint64_t>(__double_as_longlong(__dmul_rn(__ull2double_rn(a), scale)));
   return dec | (enc << 63);
+}
+
+// dequant_fp of a 64-bit code below 2^32 (a chunk whose widths are all at most
+// 32): a = ceil(enc / 2) < 2^31 never reaches the 2^52 escape, and the u32 ->
+// f64 conversion is exact, so the result equals dequant_fp's.
+__device__ __forceinline__ uint64_t dequant_fp_narrow(uint32_t enc, const QParams& q)
+{
+  if (enc == 0u) return 0ull;
+  const uint32_t a = (enc >> 1) + (enc & 1u);
+  const double scale = __longlong_as_double(static_cast<long long>(q.thr_e - 52) << 52);
+  const uint64_t dec = static_cast<uint64_t>(__double_as_longlong(__dmul_rn(__uint2double_rn(a), scale)));
+  return dec | (static_cast<uint64_t>(enc & 1u) << 63);
 }
 
 template <bool LOSSY, typename T>

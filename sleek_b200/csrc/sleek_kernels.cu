@@ -777,7 +777,10 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
   // full chunks (all but a stream's last) are unpacked without the per-value
   // bound test (f32 lossy decode +11 %); 64-bit chunks whose widths are all at
   // most 32 (typical of lossy streams) extract each value from two words
-  // instead of three (f64 lossy decode +23 %)
+  // instead of three and dequantize it in 32-bit arithmetic (f64 lossy decode
+  // +23 %, then +7-13 %).  A zero width needs no test: its mask is 0, and the
+  // words it reads lie inside the stage (the data end at most 12 bytes short
+  // of the stage's end).
   auto unpack = [&](auto full, auto narrow) {
 #pragma unroll
     for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
@@ -788,12 +791,14 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
 #pragma unroll
       for (int j = lane; j < V::VPS; j += 32) {
         if (decltype(full)::value || k0 + j < nv) {
-          T e = 0;
-          if (ln) {
+          if constexpr (sizeof(T) == 8 && LOSSY && decltype(narrow)::value) {
+            o[k0 + j] = dequant_fp_narrow(extract_bits32(w, base + j * ln, ln), q);
+          } else {
+            T e;
             if constexpr (sizeof(T) == 4 || decltype(narrow)::value) e = extract_bits32(w, base + j * ln, ln);
             else e = extract_bits64(w, base + j * ln, ln);
+            o[k0 + j] = decode_value<LOSSY>(e, q);
           }
-          o[k0 + j] = decode_value<LOSSY>(e, q);
         }
       }
     }
