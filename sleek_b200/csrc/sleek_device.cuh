@@ -165,13 +165,15 @@ __device__ __forceinline__ void set_status(uint64_t* ws, unsigned code, long lon
 // lossless forward :356-374, inverse :614-632, quantize :776-802, deQuantize
 // :1077-1108).  Bit-exactness of the stream depends on these being identical.
 // ----------------------------------------------------------------------------
+// The reference's forward step, on the rotated word v with exponent field
+// E = v >> 24: if E != 0, subtract 2^31, then subtract one more exponent unit if
+// the field became 0 or the top bit is set.  Case by case that adds 0 (E = 0),
+// 2^31 - 2^24 (1 <= E <= 0x80) or 2^31 (E > 0x80) mod 2^32, which is how it is
+// computed here (equal on all 2^32 inputs).
 __device__ __forceinline__ uint32_t fwd(uint32_t v)
 {
   v = (v << 1) | (v >> 31);
-  if (v & 0xff000000u) {
-    v -= 0x80000000u;
-    if (((v & 0xff000000u) == 0u) | (v >= 0x80000000u)) v -= 0x01000000u;
-  }
+  v += v < 0x01000000u ? 0u : (v < 0x81000000u ? 0x7f000000u : 0x80000000u);
   return (v << 1) ^ static_cast<uint32_t>(static_cast<int32_t>(v) >> 31);
 }
 
@@ -184,10 +186,8 @@ __device__ __forceinline__ uint64_t fwd(uint64_t v)
   const uint32_t l = static_cast<uint32_t>(v);
   uint32_t nh = __funnelshift_l(l, h, 1);        // rotate left by 1
   const uint32_t nl = __funnelshift_l(h, l, 1);
-  if (nh & 0xffe00000u) {
-    nh -= 0x80000000u;
-    if (((nh & 0xffe00000u) == 0u) | (nh >= 0x80000000u)) nh -= 0x00200000u;
-  }
+  // the same step on the 11-bit field: adds 0, 2^31 - 2^21 or 2^31
+  nh += nh < 0x00200000u ? 0u : (nh < 0x80200000u ? 0x7fe00000u : 0x80000000u);
   const uint32_t sg = static_cast<uint32_t>(static_cast<int32_t>(nh) >> 31);
   const uint32_t oh = __funnelshift_l(nl, nh, 1) ^ sg;  // (v << 1) ^ (v >> 63 arithmetic)
   const uint32_t ol = (nl << 1) ^ sg;
