@@ -1,12 +1,16 @@
 """Host logic of the serving loop that needs no GPU: the device-memory pool's
-first-fit allocation and coalescing, and the batch item layout."""
+next-fit allocation and coalescing, the batch item layout, and the loop's
+refusal of requests that can never be admitted (it must end, not spin)."""
 import ctypes as C
 import random
+import time
 
 import numpy as np
+import pytest
+import torch
 
 from sleek_b200 import _capi
-from sleek_b200.serve import GRANULE, ITEM_DTYPE, DevicePool
+from sleek_b200.serve import GRANULE, ITEM_DTYPE, DevicePool, Request, Server
 
 
 def test_item_layout_matches_the_c_struct():
@@ -15,7 +19,7 @@ def test_item_layout_matches_the_c_struct():
         assert ITEM_DTYPE.fields[name][1] == getattr(_capi.BatchItem, name).offset
 
 
-def test_pool_first_fit_and_coalescing():
+def test_pool_next_fit_and_coalescing():
     p = DevicePool(64 * GRANULE, device="cpu")
     a = p.alloc(10 * GRANULE)
     b = p.alloc(1)
@@ -25,9 +29,12 @@ def test_pool_first_fit_and_coalescing():
     assert p.alloc(40 * GRANULE) is None
     p.free(b, 1)
     p.free(a, 10 * GRANULE)
-    assert p.alloc(11 * GRANULE) == 0  # a and b merged
+    t = p.alloc(33 * GRANULE)  # next fit: the search starts after c
+    assert t == 31 * GRANULE
+    assert p.alloc(11 * GRANULE) == 0  # wraps around to a and b, merged
     p.free(0, 11 * GRANULE)
     p.free(c, 20 * GRANULE)
+    p.free(t, 33 * GRANULE)
     assert p.free_bytes == 64 * GRANULE
     assert p.alloc(64 * GRANULE) == 0  # everything merged back
 
@@ -50,3 +57,29 @@ def test_pool_random_alloc_free_keeps_accounting():
     for off, n in live:
         p.free(off, n)
     assert p.free_bytes == p.size and p.alloc(p.size) == 0
+
+
+def _bare_server(pool_bytes, max_batch_chunks=1 << 10):
+    """A server without CUDA streams or plans: admission and the loop's exit
+    conditions only (with no slot nothing is ever launched)."""
+    srv = Server.__new__(Server)
+    srv.pool = DevicePool(pool_bytes, device="cpu")
+    srv.max_batch, srv.max_batch_chunks = 8, max_batch_chunks
+    srv.slots, srv.queue, srv.completed = [], [], []
+    srv.t0 = time.perf_counter()
+    return srv
+
+
+def test_server_fails_what_can_never_be_admitted_and_ends():
+    srv = _bare_server(1 << 20, max_batch_chunks=16)
+    x = torch.zeros(1 << 20, dtype=torch.float32)  # 4 MB: its stream cannot fit a 1 MB pool
+    y = torch.zeros(1 << 17, dtype=torch.float32)  # 512 KB = 32 chunks: more than a launch holds
+    z = torch.zeros(1 << 10, dtype=torch.float32)  # fits, but no slot will ever run it
+    reqs = [Request("compress", t, np.dtype(np.float32), None, arrival=0.0, rid=i) for i, t in enumerate((x, y, z))]
+    stats = srv.serve(reqs)
+    assert stats["requests"] == 3 and stats["errors"] == 3
+    for r in reqs:
+        assert r.result_bytes == -_capi.SLEEK_ERR_CAPACITY
+        with pytest.raises(_capi.SleekError):
+            srv.result(r)
+    assert srv.pool.free_bytes == srv.pool.size and not srv.queue
