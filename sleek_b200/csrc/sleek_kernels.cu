@@ -184,8 +184,8 @@ __device__ __forceinline__ void pack_subchunk(uint32_t* pw, int ln, const T (&v)
   }
 }
 
-// The lane's bit run of P values of width ln as a 128-bit number x3:x2:x1:x0,
-// without branches, for 32 <= P*ln and ln < the value width.
+// The lane's bit run of four 32-bit values of width ln (8 <= ln <= 31) as a
+// 128-bit number x3:x2:x1:x0, without branches.
 __device__ __forceinline__ void run_words(const uint32_t (&v)[4], int ln, uint32_t& x0, uint32_t& x1, uint32_t& x2,
                                           uint32_t& x3)
 {
@@ -196,21 +196,6 @@ __device__ __forceinline__ void run_words(const uint32_t (&v)[4], int ln, uint32
   const int k = 2 * ln;
   const bool q = k >= 32;
   const int r = k & 31;
-  const uint32_t t0 = b0 << r, t1 = __funnelshift_l(b0, b1, r), t2 = __funnelshift_l(b1, 0u, r);
-  x0 = a0 | (q ? 0u : t0);
-  x1 = a1 | (q ? t0 : t1);
-  x2 = q ? t1 : t2;
-  x3 = q ? t2 : 0u;
-}
-
-__device__ __forceinline__ void run_words(const uint64_t (&v)[2], int ln, uint32_t& x0, uint32_t& x1, uint32_t& x2,
-                                          uint32_t& x3)
-{
-  // v0 | v1 << ln with 16 <= ln <= 63 (below 32 both values fit in 32 bits)
-  const uint32_t a0 = static_cast<uint32_t>(v[0]), a1 = static_cast<uint32_t>(v[0] >> 32);
-  const uint32_t b0 = static_cast<uint32_t>(v[1]), b1 = static_cast<uint32_t>(v[1] >> 32);
-  const bool q = ln >= 32;
-  const int r = ln & 31;
   const uint32_t t0 = b0 << r, t1 = __funnelshift_l(b0, b1, r), t2 = __funnelshift_l(b1, 0u, r);
   x0 = a0 | (q ? 0u : t0);
   x1 = a1 | (q ? t0 : t1);
@@ -239,35 +224,37 @@ __device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[
     all_short &= P * lnu[u] < 32;
   }
   if (all_long) {
+    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-    for (int g = 0; g < SPW; g += PACK_GROUP) {
-    uint32_t y[SPW][5], tl[SPW], pv[SPW];
-    int nf[SPW];
+      for (int g = 0; g < SPW; g += PACK_GROUP) {
+        uint32_t y[SPW][5], tl[SPW], pv[SPW];
+        int nf[SPW];
 #pragma unroll
-    for (int u = g; u < g + PACK_GROUP; ++u) {
-      const int R = P * lnu[u];
-      const int s = (lane * R) & 31;
-      uint32_t x0, x1, x2, x3;
-      run_words(v[u], lnu[u], x0, x1, x2, x3);
-      y[u][0] = x0 << s;
-      y[u][1] = __funnelshift_l(x0, x1, s);
-      y[u][2] = __funnelshift_l(x1, x2, s);
-      y[u][3] = __funnelshift_l(x2, x3, s);
-      y[u][4] = __funnelshift_l(x3, 0u, s);
-      nf[u] = (s + R) >> 5;
-      tl[u] = nf[u] == 1 ? y[u][1] : (nf[u] == 2 ? y[u][2] : (nf[u] == 3 ? y[u][3] : y[u][4]));
-    }
+        for (int u = g; u < g + PACK_GROUP; ++u) {
+          const int R = P * lnu[u];
+          const int s = (lane * R) & 31;
+          uint32_t x0, x1, x2, x3;
+          run_words(v[u], lnu[u], x0, x1, x2, x3);
+          y[u][0] = x0 << s;
+          y[u][1] = __funnelshift_l(x0, x1, s);
+          y[u][2] = __funnelshift_l(x1, x2, s);
+          y[u][3] = __funnelshift_l(x2, x3, s);
+          y[u][4] = __funnelshift_l(x3, 0u, s);
+          nf[u] = (s + R) >> 5;
+          tl[u] = nf[u] == 1 ? y[u][1] : (nf[u] == 2 ? y[u][2] : (nf[u] == 3 ? y[u][3] : y[u][4]));
+        }
 #pragma unroll
-    for (int u = g; u < g + PACK_GROUP; ++u) pv[u] = __shfl_up_sync(0xffffffffu, tl[u], 1);
+        for (int u = g; u < g + PACK_GROUP; ++u) pv[u] = __shfl_up_sync(0xffffffffu, tl[u], 1);
 #pragma unroll
-    for (int u = g; u < g + PACK_GROUP; ++u) {
-      const int rs = lane * P * lnu[u];
-      uint32_t* const d = pw + wbase[u] + (rs >> 5);
-      d[0] = (rs & 31) ? (y[u][0] | pv[u]) : y[u][0];
-      if (nf[u] > 1) d[1] = y[u][1];
-      if (nf[u] > 2) d[2] = y[u][2];
-      if (nf[u] > 3) d[3] = y[u][3];
-    }
+        for (int u = g; u < g + PACK_GROUP; ++u) {
+          const int rs = lane * P * lnu[u];
+          uint32_t* const d = pw + wbase[u] + (rs >> 5);
+          d[0] = (rs & 31) ? (y[u][0] | pv[u]) : y[u][0];
+          if (nf[u] > 1) d[1] = y[u][1];
+          if (nf[u] > 2) d[2] = y[u][2];
+          if (nf[u] > 3) d[3] = y[u][3];
+        }
+      }
     }
   } else if (all_short) {
     // see pack_subchunk: the first run in each word stores it, the rest OR in
