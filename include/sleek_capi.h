@@ -22,7 +22,10 @@
  * first call outside stream capture), or pass a device buffer of at least
  * sleek_*_workspace_size() bytes.  The library clears the part it uses with
  * cudaMemsetAsync on the same stream before each launch.  Calls that share one
- * workspace must be ordered on one stream.
+ * workspace must be ordered on one stream.  A library-owned workspace is replaced
+ * (after a synchronisation of its stream) when a call needs more than it holds,
+ * so host threads that issue calls on the same stream must not overlap their
+ * calls; threads on different streams need no coordination.
  */
 #ifndef SLEEK_CAPI_H
 #define SLEEK_CAPI_H
