@@ -118,6 +118,35 @@ def test_value_patterns(cuda, dt, kind):
         assert gpu_decode(s, dt, eb).tobytes() == O.decode(s, dt, eb).tobytes()
 
 
+def test_f64_lossy_width_32_boundary(cuda):
+    """64-bit lossy chunks whose widths are all at most 32 decode through 32-bit
+    extraction and dequantization: a full chunk whose widest subchunk has exactly
+    32 bits (codes up to 2^32 - 2), a 33-bit chunk in the same stream, and a
+    partial last chunk with zero-width subchunks.  With eb = 1e-3 a value's code
+    is about 2^10 |x|, so |x| in [2^21, 2^22) gives 32-bit codes."""
+    rng = np.random.default_rng(11)
+    v = 16384 // 8
+
+    def band(lo, hi, n):
+        return (rng.uniform(lo, hi, n) * np.where(rng.random(n) < 0.5, -1, 1)).astype(np.float64)
+
+    x = np.concatenate([band(2 ** 21, 2 ** 22, v), band(2 ** 22, 2 ** 23, v), band(2 ** 21, 2 ** 22, 100)])
+    x[5] = 2.0 ** 22 - 2.0 ** -9  # the largest code that still has 32 bits
+    s = gpu_encode(x, 1e-3)
+    assert s == O.encode(x, 1e-3)
+    chunks = 3
+    sizes = np.frombuffer(s[8:8 + 2 * chunks], np.uint16)
+    off, widest = 8 + 2 * chunks, []
+    for c in range(chunks):
+        ln = np.frombuffer(s[off:off + 32], np.uint8)
+        widest.append((int(ln.min()), int(ln.max())))
+        off += int(sizes[c])
+    assert widest == [(32, 32), (33, 33), (0, 32)]  # the cases this test is about
+    y = gpu_decode(s, np.float64, 1e-3)
+    assert y.tobytes() == O.decode(s, np.float64, 1e-3).tobytes()
+    assert maxabs_ok(x, y, 1e-3)
+
+
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
 @pytest.mark.parametrize("eb", [0.0, 1e-40, -1e-3, 1e-30, 1e3])
 def test_error_bound_corner_cases(cuda, dt, eb):
