@@ -460,8 +460,8 @@ __device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
 // ----------------------------------------------------------------------------
 // Decoupled look-back over flag words.  Called by one whole warp for item
 // `idx` whose segment starts at `seg_begin` (items before the segment count as
-// an inclusive prefix of 0).  Each poll reads the 128 nearest unresolved flags
-// (four independent loads per lane), sums the run of aggregates up to the
+// an inclusive prefix of 0).  Each poll reads the 32 nearest unresolved flags
+// (one load per lane), sums the run of aggregates up to the
 // nearest inclusive prefix, and slides past runs of aggregates; it only waits
 // when the nearest unresolved flag is not published yet.  Returns the exclusive
 // prefix, or -1 when a wait exceeded `limit_ns` or another CTA already
@@ -470,7 +470,7 @@ __device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
 __device__ __forceinline__ long long lookback(const uint64_t* flags, long long idx, long long seg_begin,
                                               const uint64_t* ws, unsigned long long limit_ns = SPIN_TIMEOUT_NS)
 {
-  constexpr int PER = 4;
+  constexpr int PER = 1;  // polls of 32 flags: measured against 64 and 128, encode +2 % and +4-9 %
   const int lane = threadIdx.x & 31;
   long long excl = 0;
   long long end = idx - 1;
