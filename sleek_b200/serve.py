@@ -182,11 +182,17 @@ class Server:
 
     def _take(self) -> List[Request]:
         """Admitted requests for one launch: outputs allocated from the pool, in
-        arrival order, skipping (for now) those that do not fit yet."""
+        arrival order, skipping (for now) those that do not fit yet.  Once the
+        launch is full the rest of the queue stays as it is, in one slice (a
+        burst's long queue is not walked request by request)."""
         take, chunks, keep = [], 0, []
-        for r in self.queue:
+        queue = self.queue
+        for i, r in enumerate(queue):
+            if len(take) == self.max_batch:
+                keep.extend(queue[i:])
+                break
             ch = (r.raw_bytes + 16383) // 16384
-            if len(take) < self.max_batch and chunks + ch <= self.max_batch_chunks:
+            if chunks + ch <= self.max_batch_chunks:
                 n = self._out_bytes(r)
                 off = self.pool.alloc(n)
                 if off is not None:

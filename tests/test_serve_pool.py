@@ -83,3 +83,39 @@ def test_server_fails_what_can_never_be_admitted_and_ends():
         with pytest.raises(_capi.SleekError):
             srv.result(r)
     assert srv.pool.free_bytes == srv.pool.size and not srv.queue
+
+
+def _take_by_walking(srv):
+    """The admission rule written as a walk over the whole queue (every request
+    after a full launch is kept unchanged)."""
+    take, chunks, keep = [], 0, []
+    for r in srv.queue:
+        ch = (r.raw_bytes + 16383) // 16384
+        if len(take) < srv.max_batch and chunks + ch <= srv.max_batch_chunks:
+            n = srv._out_bytes(r)
+            off = srv.pool.alloc(n)
+            if off is not None:
+                r.out_off, r.out_bytes = off, n
+                take.append(r)
+                chunks += ch
+                continue
+        keep.append(r)
+    srv.queue = keep
+    return take
+
+
+def test_take_equals_the_full_walk():
+    rng = random.Random(5)
+    src = torch.zeros(1 << 18, dtype=torch.float32)
+    for trial in range(40):
+        sizes = [rng.choice([1, 100, 5000, 40000, 200000]) for _ in range(rng.randint(1, 60))]
+        a = _bare_server(rng.choice([1 << 20, 4 << 20, 64 << 20]), max_batch_chunks=rng.choice([8, 64, 1024]))
+        b = _bare_server(a.pool.size, a.max_batch_chunks)
+        a.max_batch = b.max_batch = rng.choice([1, 3, 8, 100])
+        for srv in (a, b):
+            srv.queue = [Request("compress", src[:n], np.dtype(np.float32), None, rid=i) for i, n in enumerate(sizes)]
+        for _ in range(4):  # successive launches from the same queue and pool
+            got = [(r.rid, r.out_off) for r in a._take()]
+            want = [(r.rid, r.out_off) for r in _take_by_walking(b)]
+            assert got == want, trial
+            assert [r.rid for r in a.queue] == [r.rid for r in b.queue]
