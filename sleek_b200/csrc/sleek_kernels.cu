@@ -765,9 +765,9 @@ __device__ __forceinline__ bool decode_chunk_warp(const uint8_t* stg, int sft, i
   // bound test (f32 lossy decode +11 %); 64-bit chunks whose widths are all at
   // most 32 (typical of lossy streams) extract each value from two words
   // instead of three and dequantize it in 32-bit arithmetic (f64 lossy decode
-  // +23 %, then +7-13 %).  A zero width needs no test: its mask is 0, and the
-  // words it reads lie inside the stage (the data end at most 12 bytes short
-  // of the stage's end).
+  // +23 %, then +7-13 %).  A zero width needs no test: its mask is 0, and its
+  // reads, like every extraction's, end within 12 bytes of a bit inside the
+  // chunk's payload (at most 15 + 16383 + 10 bytes into a stage of 16384 + 64).
   auto unpack = [&](auto full, auto narrow) {
 #pragma unroll
     for (int u = 0; u < SC / NW; ++u) {  // unrolled: the subchunks' load chains overlap
