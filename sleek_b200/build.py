@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     objs = []
     for src in _sources():
         obj = os.path.join(LIB_DIR, os.path.basename(src)[:-3] + ".o")
-        cmd = ["nvcc", *NVCC_FLAGS, "-dc" if False else "-c", src, "-o", obj]
+        cmd = ["nvcc", *NVCC_FLAGS, "-c", src, "-o", obj]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:

@@ -53,6 +53,9 @@ int fill_job(const sleek_batch_item& it, int decompress, sleek::BatchJob& j)
   if (it.num_elements > 0 && (!it.input || !it.output)) return SLEEK_ERR_INVALID_ARG;
   if (!it.output || (decompress && !it.input)) return SLEEK_ERR_INVALID_ARG;
   const int w = it.elem_bytes;
+  // the largest input the single-buffer entry points accept (2^52 bytes): larger
+  // counts would overflow the byte and chunk arithmetic below
+  if (it.num_elements > (1ll << 52) / w) return SLEEK_ERR_INVALID_ARG;
   const uintptr_t in = reinterpret_cast<uintptr_t>(it.input);
   const uintptr_t out = reinterpret_cast<uintptr_t>(it.output);
   if (decompress ? ((in & 7u) || (out % w)) : ((in % w) || (out & 7u))) return SLEEK_ERR_ALIGNMENT;
@@ -124,6 +127,12 @@ int sleek_batch_plan_create(const sleek_batch_item* items, int n, int decompress
 {
   if (!plan || n < 0 || (n > 0 && !items)) return SLEEK_ERR_INVALID_ARG;
   *plan = nullptr;
+  // every item is checked before anything touches the device
+  for (int i = 0; i < n; ++i) {
+    sleek::BatchJob scratch;
+    const int rc = fill_job(items[i], decompress ? 1 : 0, scratch);
+    if (rc) return rc;
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();

@@ -114,3 +114,19 @@ def test_no_device_is_a_status_not_a_crash():
     L = _capi.lib()
     fake = 0x10000
     assert L.sleek_compress_f32(fake, 10, fake, fake, None, 0, None) == _capi.SLEEK_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("elem", [4, 8])
+def test_batch_items_beyond_the_largest_input_are_rejected_on_the_host(elem):
+    # 2^52 bytes is the largest input any entry point accepts; one element more
+    # would overflow the plan's byte and chunk arithmetic
+    L = _capi.lib()
+    fake = 0x10000  # never dereferenced: the item fails a host check first
+    it = _capi.BatchItem(fake, fake, fake, (1 << 52) // elem + 1, -1, elem, 0, 0.0)
+    plan = C.c_void_p()
+    for decompress in (0, 1):
+        rc = L.sleek_batch_plan_create(C.byref(it), 1, decompress, C.byref(plan))
+        assert rc == _capi.SLEEK_ERR_INVALID_ARG
+        assert not plan.value
+    it.num_elements = -1
+    assert L.sleek_batch_plan_create(C.byref(it), 1, 0, C.byref(plan)) == _capi.SLEEK_ERR_INVALID_ARG
