@@ -286,13 +286,11 @@ def bench_batched(dev, world, args):
     total = sum(a.numel() * a.element_size() for a in arrays)
     st = torch.cuda.current_stream()
 
-    # sequential plain launches through the C ABI, one buffer per call
+    # sequential plain launches through the C ABI, one buffer per call, with the
+    # library-owned workspace (one kernel launch per call)
     outs = [torch.empty(api.sleek_upper_bound_size(a.numel() * a.element_size()) + 16, dtype=torch.uint8,
                         device=dev) for a in arrays]
     szs = torch.zeros(len(arrays), dtype=torch.int64, device=dev)
-    wsb = max(L.sleek_compress_workspace_size(a.numel() * a.element_size()) for a in arrays)
-    wsb = max(wsb, L.sleek_decompress_workspace_size())
-    ws = torch.zeros(wsb, dtype=torch.uint8, device=dev)
     ebi = [None if eb is None else api.sleek_error_bound(eb, np.float32 if a.dtype == torch.float32
                                                          else np.float64).c_struct() for a, eb in zip(arrays, ebs)]
 
@@ -302,10 +300,10 @@ def bench_batched(dev, world, args):
             t = "f32" if a.dtype == torch.float32 else "f64"
             if ebi[i] is None:
                 rc = getattr(L, f"sleek_compress_{t}")(a.data_ptr(), a.numel(), outs[i].data_ptr(),
-                                                       szs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+                                                       szs[i:].data_ptr(), None, 0, sh)
             else:
                 rc = getattr(L, f"sleek_compress_lossy_{t}")(ebi[i], a.data_ptr(), a.numel(), outs[i].data_ptr(),
-                                                             szs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+                                                             szs[i:].data_ptr(), None, 0, sh)
             _capi.check(rc)
 
     decs = [torch.empty_like(a) for a in arrays]
@@ -318,11 +316,11 @@ def bench_batched(dev, world, args):
             cap = a.numel() * a.element_size()
             if ebi[i] is None:
                 rc = getattr(L, f"sleek_decompress_{t}")(outs[i].data_ptr(), outs[i].numel(), decs[i].data_ptr(), cap,
-                                                         dszs[i:].data_ptr(), ws.data_ptr(), wsb, sh)
+                                                         dszs[i:].data_ptr(), None, 0, sh)
             else:
                 rc = getattr(L, f"sleek_decompress_lossy_{t}")(ebi[i], outs[i].data_ptr(), outs[i].numel(),
                                                                decs[i].data_ptr(), cap, dszs[i:].data_ptr(),
-                                                               ws.data_ptr(), wsb, sh)
+                                                               None, 0, sh)
             _capi.check(rc)
 
     def graph_of(fn):
@@ -332,6 +330,7 @@ def bench_batched(dev, world, args):
         s2 = torch.cuda.Stream()
         s2.wait_stream(st)
         with torch.cuda.stream(s2):
+            fn(s2)  # outside capture: the library-owned workspace of s2 exists before it
             with torch.cuda.graph(g, stream=s2):
                 fn(s2)
         st.wait_stream(s2)
@@ -381,13 +380,76 @@ def bench_batched(dev, world, args):
     }
 
 
+def serve_plain(reqs, dev) -> dict:
+    """The per-buffer form of the served workload: every request, at its arrival
+    time, is one plain call of the reference-shaped entry points
+    (sleek_compress_* / sleek_decompress_*, library-owned workspace) on one stream;
+    a request completes when the event recorded after its call has passed.  Same
+    clock, latency and throughput definitions as Server.serve."""
+    import collections
+
+    from sleek_b200 import _capi, api
+
+    L = _capi.lib()
+    st = torch.cuda.Stream(dev)
+    sh = st.cuda_stream
+    maxraw = max(r.raw_bytes for r in reqs)
+    out = torch.empty(api.sleek_upper_bound_size(maxraw) + 16, dtype=torch.uint8, device=dev)
+    size = torch.zeros(1, dtype=torch.int64, device=dev)
+    ebc = {}
+
+    def call(r):
+        dt = np.dtype(r.dtype)
+        t = "f32" if dt == np.float32 else "f64"
+        lossy = r.eb is not None
+        if lossy and (r.eb, t) not in ebc:
+            ebc[(r.eb, t)] = api.sleek_error_bound(r.eb, dt).c_struct()
+        pre = (ebc[(r.eb, t)],) if lossy else ()
+        mid = "_lossy" if lossy else ""
+        if r.op == "compress":
+            rc = getattr(L, f"sleek_compress{mid}_{t}")(*pre, r.src.data_ptr(), r.src.numel(), out.data_ptr(),
+                                                       size.data_ptr(), None, 0, sh)
+        else:
+            rc = getattr(L, f"sleek_decompress{mid}_{t}")(*pre, r.src.data_ptr(), r.src.numel(), out.data_ptr(),
+                                                         r.num_elements * dt.itemsize, size.data_ptr(), None, 0, sh)
+        _capi.check(rc)
+
+    pending = sorted(reqs, key=lambda r: r.arrival)
+    inflight = collections.deque()
+    n = len(pending)
+    i = 0
+    t0 = time.perf_counter()
+    while i < n or inflight:
+        now = time.perf_counter() - t0
+        while i < n and pending[i].arrival <= now:
+            call(pending[i])
+            ev = torch.cuda.Event()
+            ev.record(st)
+            inflight.append((ev, pending[i]))
+            i += 1
+            if inflight[0][0].query():
+                break
+        while inflight and inflight[0][0].query():
+            inflight.popleft()[1].done = time.perf_counter() - t0
+    st.synchronize()
+    lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
+    span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+    nbytes = sum(r.raw_bytes for r in reqs)
+    return {"requests": n, "bytes": nbytes, "span_s": round(span, 4), "gbs": round(nbytes / span / 1e9, 1),
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+
+
 def bench_serve(dev, n_requests: int, seed: int = 4):
     """The served workload: Poisson arrivals at 70 % of the loop's measured peak,
     sizes log-uniform 1 KB - 256 MB, 60 / 40 compress / decompress, half lossy with
     bounds log-uniform in [1e-6, 1e-2], outputs in a device pool of up to 150 GB.
-    Decompress requests read streams made beforehand by the compressor (equal to
-    the oracle's by the parity tests).  1 % of the requests are re-run alone
-    through the single-buffer entry points and compared bit for bit."""
+    Decompress requests read one of 256 distinct streams made beforehand by the
+    compressor (about 5 GB in all, many times the 126 MB L2).  The same arrival
+    trace also runs through one plain entry-point call per request (serve_plain),
+    and both forms' peaks are measured with every request queued at once.  1 % of
+    the served requests are re-run alone through the single-buffer entry points and
+    compared bit for bit; up to 200 of them (those of at most 8 MB) are kept on the
+    host for the oracle check of the CPU-baseline leg."""
     from sleek_b200 import api
     from sleek_b200.serve import Request, Server
 
@@ -397,13 +459,21 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     src32 = (torch.cumsum(torch.randn(n_src // 4, generator=g, device=dev), 0) * 1e-3).contiguous()
     src64 = (torch.cumsum(torch.randn(n_src // 8, generator=g, device=dev, dtype=torch.float64), 0) * 1e-3)
     lo, hi = np.log(1024), np.log(256 << 20)
-    bank = []
-    for i in range(48):
-        dt = np.float32 if i % 2 else np.float64
+
+    def pick(dt):
         src = src32 if dt == np.float32 else src64
         cnt = max(1, int(np.exp(rng.uniform(lo, hi))) // np.dtype(dt).itemsize)
-        eb = None if i % 2 == 0 else float(10 ** rng.uniform(-6, -2))
-        bank.append((api.compress(src[:cnt], eb), np.dtype(dt), eb, cnt))
+        per16 = 16 // np.dtype(dt).itemsize  # request buffers start 16-byte aligned
+        off = int(rng.integers(0, (src.numel() - cnt) // per16)) * per16
+        return src[off:off + cnt]
+
+    bank = []
+    for i in range(256):
+        dt = np.float32 if i % 2 else np.float64
+        eb = None if (i // 2) % 2 == 0 else float(10 ** rng.uniform(-6, -2))
+        x = pick(dt)
+        bank.append((api.compress(x, eb), np.dtype(dt), eb, x.numel()))
+    bank_bytes = sum(b[0].numel() for b in bank)
 
     def make(n, rate):
         reqs, t = [], 0.0
@@ -411,22 +481,24 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
             t += rng.exponential(1.0 / rate) if rate else 0.0
             if rng.random() < 0.6:
                 dt = np.float32 if rng.random() < 0.5 else np.float64
-                src = src32 if dt == np.float32 else src64
-                cnt = max(1, int(np.exp(rng.uniform(lo, hi))) // np.dtype(dt).itemsize)
-                per16 = 16 // np.dtype(dt).itemsize  # request buffers start 16-byte aligned
-                off = int(rng.integers(0, (src.numel() - cnt) // per16)) * per16
+                x = pick(dt)
                 eb = None if rng.random() < 0.5 else float(10 ** rng.uniform(-6, -2))
-                reqs.append(Request("compress", src[off:off + cnt], np.dtype(dt), eb, arrival=t, rid=k))
+                reqs.append(Request("compress", x, np.dtype(dt), eb, arrival=t, rid=k))
             else:
                 st_, dt, eb, cnt = bank[int(rng.integers(0, len(bank)))]
                 reqs.append(Request("decompress", st_, dt, eb, num_elements=cnt, arrival=t, rid=k))
         return reqs
 
+    def clone(rs):
+        return [Request(r.op, r.src, r.dtype, r.eb, num_elements=r.num_elements, arrival=r.arrival, rid=r.rid)
+                for r in rs]
+
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150 << 30, free - (8 << 30)))
     srv = Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
-    # peak: everything queued at once
+    # peaks: everything queued at once, served and plain
     warm = make(min(2000, n_requests), 0.0)
+    plain_peak = serve_plain(clone(warm), dev)["gbs"]
     peak = srv.serve(warm)["gbs"]
     reqs = make(n_requests, 0.0)
     mean_bytes = np.mean([r.raw_bytes for r in reqs])
@@ -435,31 +507,86 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     for r in reqs:
         t += rng.exponential(1.0 / rate)
         r.arrival = t
+    plain_reqs = clone(reqs)
     sample = set(int(i) for i in rng.choice(len(reqs), max(1, len(reqs) // 100), replace=False))
     stats = srv.serve(reqs, keep=lambda r: r.rid in sample)
     exact = True
+    kept = []
     for r in reqs:
         if r.rid in sample:
             got = srv.result(r)
             alone = api.compress(r.src, r.eb) if r.op == "compress" else api.decompress(r.src, r.dtype, r.eb).view(
                 torch.uint8)
             exact = exact and torch.equal(got, alone)
+            if r.raw_bytes <= (8 << 20) and len(kept) < 200:
+                kept.append((r.op, r.src.cpu().numpy(), np.dtype(r.dtype), r.eb, got.cpu().numpy()))
             srv.release(r)
     srv.close()
+    del srv
+    torch.cuda.empty_cache()
+    plain = serve_plain(plain_reqs, dev)
     stats.update({"target_load": 0.7, "peak_gbs": peak, "arrival_rate_per_s": round(rate, 1),
                   "hbm_budget_bytes": budget, "sample_checked": len(sample), "sample_bit_exact": bool(exact),
+                  "decompress_bank": {"streams": len(bank), "bytes": bank_bytes},
+                  "plain": {**plain, "peak_gbs": plain_peak,
+                            "form": "one sleek_compress_*/sleek_decompress_* call per request, one stream"},
+                  "served_over_plain": {"peak": round(peak / plain_peak, 2),
+                                        "at_load_gbs": round(stats["gbs"] / plain["gbs"], 2)},
                   "workload": f"{n_requests} requests, Poisson at 70% of peak, 1 KB-256 MB log-uniform, "
                               "60/40 compress/decompress, 50% lossy eb in [1e-6,1e-2]"})
-    return stats
+    return stats, kept
 
 
-def bench_configs(dev, reps=10):
-    """The other configurations of the measurement table on the same device path:
-    compress / decompress GB/s of uncompressed bytes and the compression ratio.
-    The C-ABI calls (workspace clear + kernel) are captured `reps` times in a CUDA
-    graph and replayed between CUDA events, so small inputs measure the device, not
-    the Python call overhead; each result is checked by a round trip (exact for
-    lossless, within the bound for lossy)."""
+def served_oracle_check(kept) -> dict:
+    """Checker for the served leg (CPU-baseline leg only): the kept sample of served
+    results against the oracle."""
+    from oracle import oracle as O
+
+    ok = True
+    for op, src, dt, eb, got in kept:
+        if op == "compress":
+            ok = ok and got.tobytes() == O.encode(src.view(dt), eb)
+        else:
+            ok = ok and got.tobytes() == O.decode(src.tobytes(), dt, eb).tobytes()
+    return {"checked": len(kept), "bit_exact": bool(ok)}
+
+
+def _graph_gbs(fn, nbytes, reps, stream):
+    """GB/s of `nbytes` per call: `reps` calls captured in one CUDA graph, one warm
+    replay, then one replay between CUDA events on `stream`."""
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        for _ in range(reps):
+            fn()
+    with torch.cuda.stream(stream):  # replay() launches on the current stream
+        g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.replay()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    del g
+    return nbytes * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
+def _geomean(v):
+    v = [float(x) for x in v]
+    return float(np.exp(np.mean(np.log(v)))) if v else None
+
+
+def bench_configs(dev, peak, extra_rows=None, reps=10):
+    """Every single-buffer configuration of the measurement table on the same device
+    path, each beside a D2D copy of the same bytes (the reference's own comparison,
+    memcpy.cu:121-129, made per input by compress_decompress_inputs_single.py:228-240):
+    compress / decompress GB/s of uncompressed bytes, the compression ratio, the
+    fraction of the copy's GB/s and of the HBM roofline ((N + S) / t over the measured
+    copy bandwidth), then geomeans over every (configuration, mode) row as the
+    reference's harness takes them (:250-257).  The C-ABI calls use the library-owned
+    workspace and are captured `reps` times in a CUDA graph, replayed between CUDA
+    events, so small inputs measure the device, not the Python call overhead; each
+    result is checked by a round trip (exact for lossless, within the bound for lossy).
+    `extra_rows` adds rows measured elsewhere (the float64 field of the main leg)."""
     from sleek_b200 import _capi, api, workloads
 
     L = _capi.lib()
@@ -467,32 +594,34 @@ def bench_configs(dev, reps=10):
              ("c2a f32 1800x3600", lambda: workloads.c2a_latlon(device=dev), (None, 1e-3)),
              ("c2b f32 512^3", lambda: workloads.c2b_lognormal(device=dev), (None, 1e-3)),
              ("c2c f32 2^28", lambda: workloads.c2c_particles(device=dev), (None, 1e-3))]
-    out = {}
+    out = dict(extra_rows or {})
     side = torch.cuda.Stream(dev)
+    sh = side.cuda_stream
     for name, make, ebs in cases:
         x = make().contiguous().view(-1)
         N = x.numel() * x.element_size()
-        row = {"bytes": N}
         enc = torch.empty(api.sleek_upper_bound_size(N), dtype=torch.uint8, device=dev)
         dec = torch.empty_like(x)
         size = torch.zeros(2, dtype=torch.int64, device=dev)
-        wsz = max(L.sleek_compress_workspace_size(N), L.sleek_decompress_workspace_size())
-        ws = torch.zeros(wsz, dtype=torch.uint8, device=dev)
+        with torch.cuda.stream(side):
+            for _ in range(3):
+                dec.copy_(x)
+        memcpy = _graph_gbs(lambda: dec.copy_(x), N, reps, side)
+        row = {"bytes": N, "memcpy_d2d_gbs": round(memcpy, 1)}
         for eb in ebs:
-            sh = side.cuda_stream
             if eb is None:
                 fc = lambda: L.sleek_compress_f32(x.data_ptr(), x.numel(), enc.data_ptr(), size.data_ptr(),
-                                                  ws.data_ptr(), wsz, sh)
+                                                  None, 0, sh)
                 fd = lambda: L.sleek_decompress_f32(enc.data_ptr(), enc.numel(), dec.data_ptr(), N,
-                                                    size[1:].data_ptr(), ws.data_ptr(), wsz, sh)
+                                                    size[1:].data_ptr(), None, 0, sh)
             else:
                 e = api.sleek_error_bound(eb, np.float32).c_struct()
                 fc = lambda: L.sleek_compress_lossy_f32(e, x.data_ptr(), x.numel(), enc.data_ptr(),
-                                                        size.data_ptr(), ws.data_ptr(), wsz, sh)
+                                                        size.data_ptr(), None, 0, sh)
                 fd = lambda: L.sleek_decompress_lossy_f32(e, enc.data_ptr(), enc.numel(), dec.data_ptr(), N,
-                                                          size[1:].data_ptr(), ws.data_ptr(), wsz, sh)
+                                                          size[1:].data_ptr(), None, 0, sh)
             with torch.cuda.stream(side):
-                for _ in range(3):  # warm-up outside capture (grid sizes, attributes)
+                for _ in range(3):  # warm-up outside capture (grid sizes, attributes, workspace)
                     _capi.check(fc())
                     _capi.check(fd())
             side.synchronize()
@@ -503,28 +632,33 @@ def bench_configs(dev, reps=10):
             else:
                 fin = torch.isfinite(x)
                 assert bool(((dec[fin] - x[fin]).abs() <= eb).all()), name
-            res = {"ratio": round(N / S, 3)}
-            for lab, fn in (("compress_gbs", fc), ("decompress_gbs", fd)):
-                g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g, stream=side):
-                    for _ in range(reps):
-                        _capi.check(fn())
-                with torch.cuda.stream(side):  # replay() launches on the current stream
-                    g.replay()
-                    torch.cuda.synchronize()
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record(side)
-                    g.replay()
-                    e1.record(side)
-                torch.cuda.synchronize()
-                res[lab] = round(N * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9, 1)
-                del g
-            row[str(eb)] = res
+            cg = _graph_gbs(lambda: _capi.check(fc()), N, reps, side)
+            dg = _graph_gbs(lambda: _capi.check(fd()), N, reps, side)
+            row[str(eb)] = _mode_row(N, S, cg, dg, memcpy, peak)
         out[name] = row
-        del x, enc, dec, ws
+        del x, enc, dec
         torch.cuda.empty_cache()
-    out["timing"] = f"{reps} calls per CUDA graph replay, CUDA events"
+    rows = [r for cfg in out.values() for k, r in cfg.items() if isinstance(r, dict)]
+    out["geomean"] = {k: round(_geomean([r[k] for r in rows]), 3)
+                      for k in ("ratio", "compress_gbs", "decompress_gbs")}
+    out["geomean"]["memcpy_d2d_gbs"] = round(_geomean([c["memcpy_d2d_gbs"] for c in out.values()
+                                                      if "memcpy_d2d_gbs" in c]), 1)
+    for k in ("compress", "decompress"):
+        out["geomean"][f"frac_of_memcpy_{k}"] = round(_geomean([r["frac_of_memcpy"][k] for r in rows]), 3)
+        out["geomean"][f"roofline_frac_{k}"] = round(_geomean([r["roofline_frac"][k] for r in rows]), 3)
+    out["all_at_least_0.8_of_memcpy"] = {k: all(r["frac_of_memcpy"][k] >= 0.8 for r in rows)
+                                         for k in ("compress", "decompress")}
+    out["timing"] = f"{reps} calls per CUDA graph replay, CUDA events; copy: {reps} D2D copies of the same bytes"
     return out
+
+
+def _mode_row(N, S, cg, dg, memcpy, peak):
+    """One (configuration, mode) row: GB/s of N, fraction of the D2D copy and of the
+    HBM roofline ((N + S) bytes moved per call over the measured copy bandwidth)."""
+    return {"ratio": round(N / S, 3), "compress_gbs": round(cg, 1), "decompress_gbs": round(dg, 1),
+            "frac_of_memcpy": {"compress": round(cg / memcpy, 3), "decompress": round(dg / memcpy, 3)},
+            "roofline_frac": {"compress": round(cg * (N + S) / N / peak, 3),
+                              "decompress": round(dg * (N + S) / N / peak, 3)}}
 
 
 def bench_transfer(x, modes=(None, 1e-2, 1e-4), repeats=3):
@@ -606,6 +740,7 @@ def main():
 
     from sleek_b200 import _capi, api, workloads
 
+    peak, peak_kind = peaks()
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     L = _capi.lib()
@@ -619,26 +754,24 @@ def main():
     esz = torch.zeros(len(MODES), dtype=torch.int64, device=dev)
     dsz = torch.zeros(len(MODES), dtype=torch.int64, device=dev)
     dec = torch.empty_like(x)
-    wsz = max(L.sleek_compress_workspace_size(N), L.sleek_decompress_workspace_size())
-    ws = torch.zeros(wsz, dtype=torch.uint8, device=dev)
     ebi = [None if eb is None else api.sleek_error_bound(eb, np.float64).c_struct() for eb in MODES]
 
+    # the reference-shaped entry points with the library-owned workspace (NULL): the
+    # kernels keep it ready themselves, so a call is one kernel launch
     def launch_c(i):
         if ebi[i] is None:
-            rc = L.sleek_compress_f64(x.data_ptr(), x.numel(), enc[i].data_ptr(), esz[i:].data_ptr(),
-                                      ws.data_ptr(), wsz, sh)
+            rc = L.sleek_compress_f64(x.data_ptr(), x.numel(), enc[i].data_ptr(), esz[i:].data_ptr(), None, 0, sh)
         else:
             rc = L.sleek_compress_lossy_f64(ebi[i], x.data_ptr(), x.numel(), enc[i].data_ptr(),
-                                            esz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+                                            esz[i:].data_ptr(), None, 0, sh)
         _capi.check(rc, "compress")
 
     def launch_d(i):
         if ebi[i] is None:
-            rc = L.sleek_decompress_f64(enc[i].data_ptr(), cap, dec.data_ptr(), N, dsz[i:].data_ptr(),
-                                        ws.data_ptr(), wsz, sh)
+            rc = L.sleek_decompress_f64(enc[i].data_ptr(), cap, dec.data_ptr(), N, dsz[i:].data_ptr(), None, 0, sh)
         else:
             rc = L.sleek_decompress_lossy_f64(ebi[i], enc[i].data_ptr(), cap, dec.data_ptr(), N,
-                                              dsz[i:].data_ptr(), ws.data_ptr(), wsz, sh)
+                                              dsz[i:].data_ptr(), None, 0, sh)
         _capi.check(rc, "decompress")
 
     # correctness gate before timing: every mode round-trips and sizes are sane
@@ -775,7 +908,6 @@ def main():
         assert got == list(S), (got, S)
 
     # ---- roofline of the dominant kernel ----------------------------------------------
-    peak, peak_kind = peaks()
     t_enc = sum(tc)
     t_dec = sum(td)
     dom = "encode" if t_enc >= t_dec else "decode"
@@ -818,18 +950,25 @@ def main():
         del enc, dec, d_in, d_out, hin, hout, hstream
         torch.cuda.empty_cache()
         line["batched"] = bench_batched(dev, world, args)
+    kept = []
     if args.serve_requests > 0:
         torch.cuda.empty_cache()
-        line["served"] = bench_serve(dev, args.serve_requests)
+        line["served"], kept = bench_serve(dev, args.serve_requests)
     if not args.no_transfer:
         line["transfer"] = bench_transfer(x)
     if not args.no_configs:
-        line["configs"] = bench_configs(dev)
+        c1_row = {"bytes": N, "memcpy_d2d_gbs": round(memcpy_gbs, 1)}
+        for i, m in enumerate(MODES):
+            c1_row[str(m)] = _mode_row(N, S[i], N / (tc[i] * 1e-3) / 1e9, N / (td[i] * 1e-3) / 1e9, memcpy_gbs, peak)
+        line["configs"] = bench_configs(dev, peak, {"c1 f64 256x384x384 (main leg, per-call CUDA events)": c1_row})
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference's own implementations on this box: its CPU codec (the baseline)
-        # and, beside it, its GPU kernels built for sm_100a
+        # and, beside it, its GPU kernels built for sm_100a; the oracle checks the
+        # kept sample of served results
         line["cpu_baseline"] = cpu_baseline(x.cpu().numpy())
         line["reference_gpu"] = reference_gpu_kernels(x)
+        if kept:
+            line["served"]["sample_oracle"] = served_oracle_check(kept)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -20,12 +20,17 @@
  * Workspace: pass NULL to use a workspace the library owns (one per device and
  * stream, grown on demand -- growth calls cudaMalloc, so size it up front with a
  * first call outside stream capture), or pass a device buffer of at least
- * sleek_*_workspace_size() bytes.  The library clears the part it uses with
- * cudaMemsetAsync on the same stream before each launch.  Calls that share one
- * workspace must be ordered on one stream.  A library-owned workspace is replaced
- * (after a synchronisation of its stream) when a call needs more than it holds,
- * so host threads that issue calls on the same stream must not overlap their
- * calls; threads on different streams need no coordination.
+ * sleek_*_workspace_size() bytes.  A caller's workspace is cleared with
+ * cudaMemsetAsync on the same stream before each launch.  The library's own
+ * workspace is cleared once, when it is allocated, and then kept ready by the
+ * kernels themselves (each launch leaves the half it did not use clean for the
+ * next), so calls with NULL issue no clearing work.  Calls that share one
+ * workspace must be ordered on one stream; a CUDA graph that holds calls with the
+ * library-owned workspace of a stream must run in that stream's order.  A
+ * library-owned workspace is replaced (after a synchronisation of its stream)
+ * when a call needs more than it holds, so host threads that issue calls on the
+ * same stream must not overlap their calls; threads on different streams need no
+ * coordination.
  */
 #ifndef SLEEK_CAPI_H
 #define SLEEK_CAPI_H
@@ -123,19 +128,39 @@ int sleek_decompress_lossy_f64(sleek_eb_info_f64 eb, const unsigned char* d_enco
  * file-scope device array inside the library (512 KiB per device, held until the process
  * exits), so inputs are limited to SLEEK_STATIC_MAX_INPUT_BYTES (1 GiB); larger ones are
  * rejected with SLEEK_ERR_TOO_LARGE.  The first call on a device looks up the scratch's
- * device address (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  All calls share the one scratch and it keeps the last call's
- * contents (each call clears what it needs on `stream`), so calls whose executions overlap
- * on the GPU (different streams, no ordering between them) race: order them on one stream.
- * Output, stream format and errors are those of sleek_compress_f32. */
+ * device address (cudaGetSymbolAddress, with that device current); with lazy module
+ * loading that lookup may load the library's device code, a one-time device allocation
+ * and possibly a synchronisation, so make that first call at initialisation time, before
+ * any stream capture.  The address is cached per device: calls must not span a
+ * cudaDeviceReset of that device.  All calls share the one scratch and it keeps the last
+ * call's contents (each call clears what it needs on `stream`), so calls whose executions
+ * overlap on the GPU (different streams, no ordering between them) race: order them on
+ * one stream.  Output, stream format and host-detected errors are those of
+ * sleek_compress_f32; a device-detected error shows only as -status in *d_encsize
+ * (sleek_workspace_status does not read the static scratch). */
 #define SLEEK_STATIC_MAX_INPUT_BYTES (1ll << 30)
 int sleek_compress_f32_static(const float* d_input, long long num_elements, unsigned char* d_encoded,
                               long long* d_encsize, void* stream);
 
 /* Tuning: CTAs per SM used by the single-buffer entry points of one kind on the current
- * device (0 = as many as fit, the default).  Set by sleek_b200.autotune; no counterpart
- * in the reference, whose grid size comes from sleek_thread_blocks. */
+ * device, for every input size (0 = as many as fit, the default).  Set by
+ * sleek_b200.autotune; no counterpart in the reference, whose grid size comes from
+ * sleek_thread_blocks and whose block size is the constant SLEEK_TPB
+ * (include/sleek_common_gpu.h:54-56, 108-119). */
 int sleek_set_ctas_per_sm(int decompress, int elem_bytes, int lossy, int ctas_per_sm);
+
+/* Tuning: launch shapes.  The single-buffer kernels are built in a few shapes (threads per
+ * CTA, compute warps, shared-memory chunk stages, and the CTAs per SM their registers are
+ * budgeted for); shape 0 is the default, and every shape writes the same bytes.
+ * sleek_launch_shape_info describes shape `shape` of the compress (decompress = 0) or
+ * decompress kernels (any output pointer may be NULL) and returns SLEEK_ERR_INVALID_ARG
+ * past the last one.  sleek_set_launch_shape selects the shape and the CTAs per SM (0 = as
+ * many as fit) of the single-buffer calls of one kind on the current device for inputs of
+ * [2^size_log2, 2^(size_log2 + 1)) bytes -- decompress: the decoded size, taken from
+ * decoded_capacity, else encoded_bytes -- or for every size with size_log2 = -1.  Set by
+ * sleek_b200.autotune from timings on the caller's data. */
+int sleek_launch_shape_info(int decompress, int shape, int* threads, int* warps, int* stages, int* ctas_per_sm);
+int sleek_set_launch_shape(int decompress, int elem_bytes, int lossy, int size_log2, int shape, int ctas_per_sm);
 
 /* ---- batched compress / decompress ---------------------------------------------
  * Many buffers of uneven sizes with mixed float32 / float64 and mixed error bounds in
@@ -255,6 +280,25 @@ const char* sleek_stream_reason_string(int reason);
  * (-1 when it gave up), h_result[2] = nanoseconds both waits took.  Synchronous on
  * the legacy default stream; the device stays usable. */
 int sleek_selftest_bounded_waits(long long limit_ns, long long* h_result);
+
+/* Self-test of the device value maps (no counterpart in the reference): on the current
+ * device, compares what the codec kernels compute -- the lossless transform and its
+ * inverse, quantize and dequantize (whose rounding division runs in floating point) --
+ * with a literal restatement of the reference's integer steps (include/sleek_common_gpu.h:
+ * forward :356-374, inverse :614-632, quantize :776-802, dequantize :1077-1108).
+ * Checks, in h_counts[0..SLEEK_SELFTEST_VALUE_CHECKS-1]:
+ *   0  float32 transform and inverse, every 32-bit word
+ *   1  float32 quantize, every word, error-bound exponents 0 1 2 24 100 127 200 230
+ *   2  float32 dequantize, every code, the same exponents
+ *   3  float64 transform and inverse, every sign/exponent field x 2^20 seeded mantissas
+ *   4  float64 quantize, the same words, error-bound exponents 0 1 2 53 500 1000 1023 1500 1993
+ *   5  float64 dequantize, every code below 2^32 (also the narrow form) and 2^32 codes
+ *      spread over every bit length, the same exponents
+ * Each entry receives the number of mismatching inputs (0 when the maps agree), and
+ * h_first (optional) the first failing index of each check (-1 if none).  Synchronous
+ * on the legacy default stream, well under a second on a B200. */
+#define SLEEK_SELFTEST_VALUE_CHECKS 6
+int sleek_selftest_value_maps(long long* h_counts, long long* h_first);
 
 /* Value range of a device array, NaNs ignored: *h_min and *h_max (host memory)
  * receive its smallest and largest value (NaN when the array has no non-NaN

@@ -25,6 +25,7 @@ SLEEK_ERR_WORKSPACE = 7
 SLEEK_ERR_NO_DEVICE = 8
 SLEEK_ERR_CAPACITY = 9
 SLEEK_ERR_TOO_LARGE = 10
+SLEEK_SELFTEST_VALUE_CHECKS = 6
 
 
 class EbInfoF32(C.Structure):
@@ -70,6 +71,9 @@ SIGNATURES = {
     "sleek_workspace_status": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "sleek_compress_f32_static": (C.c_int, [_vp, _i64, _vp, _vp, _vp]),
     "sleek_set_ctas_per_sm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "sleek_launch_shape_info": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sleek_set_launch_shape": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "sleek_compress_to_host": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_double, _vp, C.c_longlong,
                                          C.POINTER(C.c_longlong), C.c_longlong, _vp]),
     "sleek_decompress_from_host": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_double, _vp, C.c_longlong,
@@ -77,6 +81,7 @@ SIGNATURES = {
     "sleek_validate_stream": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "sleek_stream_reason_string": (C.c_char_p, [C.c_int]),
     "sleek_selftest_bounded_waits": (C.c_int, [C.c_longlong, C.POINTER(C.c_longlong)]),
+    "sleek_selftest_value_maps": (C.c_int, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "sleek_minmax_f32": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp]),
     "sleek_minmax_f64": (C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double), _vp]),
     "sleek_batch_plan_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),

@@ -2,17 +2,27 @@
 
 The 16 KB chunk is part of the stream format (``SLEEK_CS``, enforced by
 ``sleek_system_checks`` in the reference), so what is tuned is how the work is
-laid on the GPU: CTAs per SM of the persistent kernels (each CTA is 10 warps and
-keeps a 4-deep pipeline of chunks), for the single-buffer kernels of each kind and
-for batched plans.  Candidates are timed with CUDA events on the caller's data
-(outputs are identical for every candidate), and the winner is cached per device
-name and workload key in a JSON file.
+laid on the GPU, where the reference uses fixed constants (``SLEEK_TPB`` = 512
+threads and a grid from ``sleek_thread_blocks``, include/sleek_common_gpu.h:54-56,
+108-119):
+
+- single-buffer calls: the kernel shape -- threads per CTA, compute warps (and so
+  subchunks per warp) and shared-memory chunk stages, from the shapes the library
+  is built with (``sleek_launch_shape_info``) -- and the CTAs per SM, per kind
+  (element size, lossless / lossy, compress / decompress) and per input-size
+  bucket (base-2 logarithm of the bytes), applied with ``sleek_set_launch_shape``;
+- batched plans: CTAs per SM (``sleek_batch_plan_set_grid``).
+
+Candidates are timed with CUDA events on the caller's data (outputs are identical
+for every candidate), and the winner is cached per device name and key in a JSON
+file.
 """
 from __future__ import annotations
 
+import ctypes as C
 import json
 import os
-from typing import Callable, Dict, Optional
+from typing import Callable, Dict, List, Optional, Sequence
 
 import torch
 
@@ -26,7 +36,7 @@ def _cache_path() -> str:
                           os.path.join(os.path.expanduser("~"), ".cache", "sleek_b200", "tuning.json"))
 
 
-def _load() -> Dict[str, int]:
+def _load() -> Dict[str, object]:
     try:
         with open(_cache_path()) as f:
             return json.load(f)
@@ -34,7 +44,7 @@ def _load() -> Dict[str, int]:
         return {}
 
 
-def _save(d: Dict[str, int]) -> None:
+def _save(d: Dict[str, object]) -> None:
     p = _cache_path()
     os.makedirs(os.path.dirname(p), exist_ok=True)
     with open(p, "w") as f:
@@ -54,42 +64,77 @@ def _time(fn: Callable[[], None], reps: int = 5) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def tune(key: str, run_with: Callable[[int], None], candidates=CANDIDATES, use_cache: bool = True) -> dict:
-    """Times ``run_with(ctas_per_sm)`` for each candidate and returns
-    {"best": c, "ms": {c: ms}}; cached under ``key`` + device name."""
+def tune(key: str, run_with: Callable, candidates: Sequence = CANDIDATES, use_cache: bool = True) -> dict:
+    """Times ``run_with(candidate)`` for each candidate and returns
+    {"best": c, "ms": {str(c): ms}}; cached under ``key`` + device name."""
     full = f"{torch.cuda.get_device_name()}|{key}"
     cache = _load() if use_cache else {}
     if full in cache:
-        return {"best": cache[full], "ms": {}, "cached": True}
+        best = cache[full]
+        return {"best": tuple(best) if isinstance(best, list) else best, "ms": {}, "cached": True}
     ms = {c: _time(lambda c=c: run_with(c)) for c in candidates}
     best = min(ms, key=ms.get)
     if use_cache:
-        cache[full] = best
+        cache[full] = list(best) if isinstance(best, tuple) else best
         _save(cache)
-    return {"best": best, "ms": ms, "cached": False}
+    return {"best": best, "ms": {str(c): round(v, 4) for c, v in ms.items()}, "cached": False}
+
+
+def shapes(decompress: bool) -> List[dict]:
+    """The launch shapes the library is built with for one direction."""
+    L = _capi.lib()
+    out = []
+    k = 0
+    while True:
+        t, w, s, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        if L.sleek_launch_shape_info(int(decompress), k, C.byref(t), C.byref(w), C.byref(s), C.byref(c)) != 0:
+            return out
+        out.append({"shape": k, "threads": t.value, "warps": w.value, "stages": s.value, "ctas_per_sm": c.value})
+        k += 1
+
+
+def single_candidates(decompress: bool) -> List[tuple]:
+    """(shape, CTAs per SM) pairs: every shape at as many CTAs as fit (0) and at one fewer."""
+    out = []
+    for sh in shapes(decompress):
+        out.append((sh["shape"], 0))
+        if sh["ctas_per_sm"] > 1:
+            out.append((sh["shape"], sh["ctas_per_sm"] - 1))
+    return out
+
+
+def size_log2(nbytes: int) -> int:
+    return max(0, int(nbytes).bit_length() - 1)
 
 
 def tune_single(x: torch.Tensor, eb: Optional[float], decompress: bool = False, use_cache: bool = True) -> dict:
-    """Tunes and applies CTAs per SM for the single-buffer kernel of x's kind."""
+    """Tunes and applies the launch shape and CTAs per SM of the single-buffer kernel
+    of x's kind for inputs in x's size bucket."""
     from . import api
 
     L = _capi.lib()
     w = x.element_size()
     lossy = int(eb is not None)
+    nbytes = x.numel() * w
+    bucket = size_log2(nbytes)
     enc = api.compress(x, eb)
     dt = torch.float32 if w == 4 else torch.float64
     out = torch.empty_like(x)
 
+    def apply(c):
+        _capi.check(L.sleek_set_launch_shape(int(decompress), w, lossy, bucket, c[0], c[1]), "sleek_set_launch_shape")
+
     def run(c):
-        L.sleek_set_ctas_per_sm(int(decompress), w, lossy, c)
+        apply(c)
         if decompress:
             api.decompress(enc, dt, eb, out=out)
         else:
             api.compress(x, eb)
 
-    key = f"single|{'dec' if decompress else 'enc'}|{w}|{lossy}|{x.numel() * w >> 24}"
-    r = tune(key, run, use_cache=use_cache)
-    L.sleek_set_ctas_per_sm(int(decompress), w, lossy, r["best"])
+    key = f"single|{'dec' if decompress else 'enc'}|{w}|{lossy}|2^{bucket}"
+    r = tune(key, run, single_candidates(decompress), use_cache=use_cache)
+    apply(r["best"])
+    r.update({"bucket_log2": bucket, "shape": shapes(decompress)[r["best"][0]]})
     return r
 
 

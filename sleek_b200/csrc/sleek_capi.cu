@@ -17,17 +17,47 @@
 namespace {
 
 constexpr long long CS = 16384;
-constexpr int HDR_WORDS = 32;  // workspace header words, as in sleek_device.cuh
+// workspace header layout, as in sleek_device.cuh (WsWord)
+constexpr int HDR_WORDS = 32;
+constexpr int WS_STATUS = 2;
+constexpr int WS_BLOCK = 8;
+constexpr int WS_EPOCH = 16;
+constexpr int WS_MINMAX = 24;
+
+constexpr int SHAPES_MAX = 4;
+constexpr int BUCKETS = 64;  // input sizes by their base-2 logarithm
+
+// what the single-buffer calls of one kind launch for one size bucket
+struct Choice {
+  int shape = 0;  // launch shape (sleek_kernels.cu: EncShape*, DecShape*)
+  int ctas = 0;   // CTAs per SM, 0 = as many as fit
+};
 
 struct DeviceInfo {
   int sms = 0;
-  int bps[2][2][2] = {};       // [width==8][lossy][enc]: CTAs per SM that fit
-  int override_[2][2][2] = {};  // tuned CTAs per SM (0 = as many as fit)
+  int bps[2][2][2][SHAPES_MAX] = {};  // [width==8][lossy][enc][shape]: CTAs per SM that fit
+  Choice choice[2][2][2][BUCKETS];    // [width==8][lossy][enc][size bucket]
+};
+
+int size_bucket(long long bytes)
+{
+  if (bytes <= 0) return 0;
+  int b = 0;
+  while (b < BUCKETS - 1 && (bytes >> (b + 1)) != 0) ++b;
+  return b;
+}
+
+// A library-owned workspace: zeroed once when allocated, then kept clean by the
+// kernels themselves (two counter blocks and two flag regions used by alternate
+// launches, see WsPhase in sleek_device.cuh), so calls need no clearing pass.
+struct OwnedWs {
+  void* ptr = nullptr;
+  long long flag_cap = 0;  // flags per region
 };
 
 std::mutex g_mu;
 std::map<int, DeviceInfo> g_dev;
-std::map<std::pair<int, cudaStream_t>, std::pair<void*, size_t>> g_ws;
+std::map<std::pair<int, cudaStream_t>, OwnedWs> g_ws;
 
 int current_device(int* dev)
 {
@@ -38,7 +68,9 @@ int current_device(int* dev)
   return SLEEK_OK;
 }
 
-int persistent_grid(int dev, int width, bool lossy, bool enc)
+// Persistent grid and launch shape of a single-buffer call of `bytes` bytes
+// (bytes < 0: unknown, the default shape).
+int persistent_grid(int dev, int width, bool lossy, bool enc, long long bytes, int* shape)
 {
   std::lock_guard<std::mutex> lk(g_mu);
   DeviceInfo& d = g_dev[dev];
@@ -47,67 +79,83 @@ int persistent_grid(int dev, int width, bool lossy, bool enc)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     d.sms = sms > 0 ? sms : 1;
   }
-  int& b = d.bps[width == 8][lossy][enc];
+  const Choice c = bytes < 0 ? Choice{} : d.choice[width == 8][lossy][enc][size_bucket(bytes)];
+  int& b = d.bps[width == 8][lossy][enc][c.shape];
   if (b == 0) {
-    const int n = sleek::blocks_per_sm(width, lossy, enc);
+    const int n = sleek::blocks_per_sm(width, lossy, enc, c.shape);
     b = n > 0 ? n : 1;
   }
-  const int o = d.override_[width == 8][lossy][enc];
-  return d.sms * ((o > 0 && o < b) ? o : b);
+  *shape = c.shape;
+  return d.sms * ((c.ctas > 0 && c.ctas < b) ? c.ctas : b);
 }
 
-// library-owned workspace for (device, stream); grows, never shrinks
-int owned_workspace(int dev, cudaStream_t st, size_t need, void** ptr)
+// library-owned workspace for (device, stream) with room for `need_flags` flags per
+// region; grows, never shrinks.  A new one is zeroed on `st` (the only clearing it
+// ever needs).
+int owned_workspace(int dev, cudaStream_t st, long long need_flags, OwnedWs* out)
 {
   std::lock_guard<std::mutex> lk(g_mu);
-  auto& e = g_ws[{dev, st}];
-  if (e.second < need) {
-    if (e.first) {
+  OwnedWs& e = g_ws[{dev, st}];
+  if (e.ptr == nullptr || e.flag_cap < need_flags) {
+    if (e.ptr) {
       cudaStreamSynchronize(st);
-      cudaFree(e.first);
-      e.first = nullptr;
-      e.second = 0;
+      cudaFree(e.ptr);
+      e.ptr = nullptr;
+      e.flag_cap = 0;
     }
-    size_t sz = 1 << 20;
-    while (sz < need) sz <<= 1;
+    long long cap = 1 << 10;  // flags per region: 16 MB of input, doubling as needed
+    while (cap < need_flags) cap <<= 1;
+    const size_t bytes = static_cast<size_t>(8 * (HDR_WORDS + 2 * cap));
     void* p = nullptr;
-    if (cudaMalloc(&p, sz) != cudaSuccess) {
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
       cudaGetLastError();
       return SLEEK_ERR_CUDA;
     }
-    e.first = p;
-    e.second = sz;
+    if (cudaMemsetAsync(p, 0, bytes, st) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(p);
+      return SLEEK_ERR_CUDA;
+    }
+    e.ptr = p;
+    e.flag_cap = cap;
   }
-  *ptr = e.first;
+  *out = e;
   return SLEEK_OK;
 }
 
-int prepare_workspace(cudaStream_t st, void* user_ws, size_t user_bytes, size_t need, uint64_t** ws)
+// The workspace of one single-buffer launch that uses `need_flags` look-back flags:
+// the library-owned one of (device, stream) when user_ws is NULL (no clearing: it
+// resets itself), else the caller's, checked and cleared on `st` (epoch 0, so only
+// the first flag region is used).
+int prepare_workspace(cudaStream_t st, void* user_ws, size_t user_bytes, long long need_flags, uint64_t** ws,
+                      long long* flag_cap)
 {
   int dev = 0;
   int rc = current_device(&dev);
   if (rc) return rc;
-  void* p = user_ws;
-  if (p == nullptr) {
-    rc = owned_workspace(dev, st, need, &p);
+  if (user_ws == nullptr) {
+    OwnedWs o;
+    rc = owned_workspace(dev, st, need_flags, &o);
     if (rc) return rc;
-  } else {
-    if (user_bytes < need) return SLEEK_ERR_WORKSPACE;
-    if (reinterpret_cast<uintptr_t>(p) & 7u) return SLEEK_ERR_ALIGNMENT;
+    *ws = static_cast<uint64_t*>(o.ptr);
+    *flag_cap = o.flag_cap;
+    return SLEEK_OK;
   }
-  if (cudaMemsetAsync(p, 0, need, st) != cudaSuccess) {
+  const size_t need = static_cast<size_t>(8 * (HDR_WORDS + need_flags));
+  if (user_bytes < need) return SLEEK_ERR_WORKSPACE;
+  if (reinterpret_cast<uintptr_t>(user_ws) & 7u) return SLEEK_ERR_ALIGNMENT;
+  if (cudaMemsetAsync(user_ws, 0, need, st) != cudaSuccess) {
     cudaGetLastError();
     return SLEEK_ERR_CUDA;
   }
-  *ws = static_cast<uint64_t*>(p);
+  *ws = static_cast<uint64_t*>(user_ws);
+  *flag_cap = need_flags;
   return SLEEK_OK;
 }
 
-size_t enc_ws_bytes(long long insize)
-{
-  const long long chunks = (insize + CS - 1) / CS;
-  return static_cast<size_t>(8 * (HDR_WORDS + chunks));
-}
+long long enc_flags(long long insize) { return (insize + CS - 1) / CS; }
+
+size_t enc_ws_bytes(long long insize) { return static_cast<size_t>(8 * (HDR_WORDS + enc_flags(insize))); }
 
 size_t dec_ws_bytes(int grid) { return static_cast<size_t>(8 * (HDR_WORDS + grid)); }
 
@@ -126,7 +174,8 @@ int do_compress(int width, bool lossy, sleek::QParams q, const void* in, long lo
   const long long insize = n * width;
   const long long chunks = (insize + CS - 1) / CS;
   uint64_t* w = nullptr;
-  rc = prepare_workspace(st, ws, wsb, enc_ws_bytes(insize), &w);
+  long long cap = 0;
+  rc = prepare_workspace(st, ws, wsb, enc_flags(insize), &w, &cap);
   if (rc) return rc;
   sleek::EncArgs a;
   a.in = static_cast<const uint8_t*>(in);
@@ -134,10 +183,12 @@ int do_compress(int width, bool lossy, sleek::QParams q, const void* in, long lo
   a.out = out;
   a.outsize = outsize;
   a.ws = w;
+  a.flag_cap = cap;
   a.q = q;
-  long long grid = persistent_grid(dev, width, lossy, true);
+  int shape = 0;
+  long long grid = persistent_grid(dev, width, lossy, true, insize, &shape);
   if (grid > chunks) grid = chunks > 0 ? chunks : 1;
-  if (sleek::launch_encode(width, lossy, a, static_cast<int>(grid), st) != cudaSuccess) {
+  if (sleek::launch_encode(width, lossy, shape, a, static_cast<int>(grid), st) != cudaSuccess) {
     cudaGetLastError();
     return SLEEK_ERR_CUDA;
   }
@@ -156,9 +207,11 @@ int do_decompress(int width, bool lossy, sleek::QParams q, const unsigned char* 
   int rc = current_device(&dev);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int grid = persistent_grid(dev, width, lossy, false);
+  int shape = 0;
+  const int grid = persistent_grid(dev, width, lossy, false, out_cap >= 0 ? out_cap : in_len, &shape);
   uint64_t* w = nullptr;
-  rc = prepare_workspace(st, ws, wsb, dec_ws_bytes(grid), &w);
+  long long cap = 0;
+  rc = prepare_workspace(st, ws, wsb, grid, &w, &cap);
   if (rc) return rc;
   sleek::DecArgs a;
   a.in = in;
@@ -167,8 +220,9 @@ int do_decompress(int width, bool lossy, sleek::QParams q, const unsigned char* 
   a.out_cap = out_cap < 0 ? -1 : out_cap;
   a.outsize = outsize;
   a.ws = w;
+  a.flag_cap = cap;
   a.q = q;
-  if (sleek::launch_decode(width, lossy, a, grid, st) != cudaSuccess) {
+  if (sleek::launch_decode(width, lossy, shape, a, grid, st) != cudaSuccess) {
     cudaGetLastError();
     return SLEEK_ERR_CUDA;
   }
@@ -234,9 +288,15 @@ int minmax(const F* in, long long n, F* h_min, F* h_max, void* stream)
   int dev = 0;
   int rc = current_device(&dev);
   if (rc) return rc;
-  uint64_t* w = nullptr;
-  rc = prepare_workspace(st, nullptr, 0, 8 * 3, &w);  // the two keys and a clear status word
+  // the two keys live in the range-reduction words of the library-owned workspace
+  OwnedWs o;
+  rc = owned_workspace(dev, st, 0, &o);
   if (rc) return rc;
+  uint64_t* const w = static_cast<uint64_t*>(o.ptr) + WS_MINMAX;
+  if (cudaMemsetAsync(w, 0, 16, st) != cudaSuccess) {
+    cudaGetLastError();
+    return SLEEK_ERR_CUDA;
+  }
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   unsigned long long keys[2] = {0ull, 0ull};
@@ -308,7 +368,8 @@ int sleek_thread_blocks(void)
 {
   int dev = 0;
   if (current_device(&dev)) return 0;
-  return persistent_grid(dev, 4, false, true);
+  int shape = 0;
+  return persistent_grid(dev, 4, false, true, -1, &shape);
 }
 
 size_t sleek_compress_workspace_size(long long insize) { return insize < 0 ? 0 : enc_ws_bytes(insize); }
@@ -316,13 +377,17 @@ size_t sleek_compress_workspace_size(long long insize) { return insize < 0 ? 0 :
 size_t sleek_decompress_workspace_size(void)
 {
   int dev = 0;
-  if (current_device(&dev)) return dec_ws_bytes(148 * 8);
+  if (current_device(&dev)) return dec_ws_bytes(148 * 32);
+  // the largest persistent grid of any decode kind and shape
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int g = 0;
   for (int w = 4; w <= 8; w += 4)
-    for (int l = 0; l < 2; l++) {
-      const int x = persistent_grid(dev, w, l != 0, false);
-      g = x > g ? x : g;
-    }
+    for (int l = 0; l < 2; l++)
+      for (int sh = 0; sh < sleek::shape_count(false); ++sh) {
+        const int x = (sms > 0 ? sms : 1) * sleek::blocks_per_sm(w, l != 0, false, sh);
+        g = x > g ? x : g;
+      }
   return dec_ws_bytes(g);
 }
 
@@ -413,7 +478,33 @@ int sleek_set_ctas_per_sm(int decompress, int elem_bytes, int lossy, int ctas_pe
   const int rc = current_device(&dev);
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(g_mu);
-  g_dev[dev].override_[elem_bytes == 8][lossy != 0][decompress == 0] = ctas_per_sm;
+  for (Choice& c : g_dev[dev].choice[elem_bytes == 8][lossy != 0][decompress == 0]) c.ctas = ctas_per_sm;
+  return SLEEK_OK;
+}
+
+int sleek_launch_shape_info(int decompress, int shape, int* threads, int* warps, int* stages, int* ctas_per_sm)
+{
+  if (shape < 0 || shape >= sleek::shape_count(decompress == 0)) return SLEEK_ERR_INVALID_ARG;
+  const sleek::ShapeInfo i = sleek::shape_info(decompress == 0, shape);
+  if (threads) *threads = i.threads;
+  if (warps) *warps = i.warps;
+  if (stages) *stages = i.stages;
+  if (ctas_per_sm) *ctas_per_sm = i.ctas_per_sm;
+  return SLEEK_OK;
+}
+
+int sleek_set_launch_shape(int decompress, int elem_bytes, int lossy, int size_log2, int shape, int ctas_per_sm)
+{
+  if ((elem_bytes != 4 && elem_bytes != 8) || ctas_per_sm < 0 || size_log2 < -1 || size_log2 >= BUCKETS ||
+      shape < 0 || shape >= sleek::shape_count(decompress == 0))
+    return SLEEK_ERR_INVALID_ARG;
+  int dev = 0;
+  const int rc = current_device(&dev);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_mu);
+  Choice* row = g_dev[dev].choice[elem_bytes == 8][lossy != 0][decompress == 0];
+  for (int b = 0; b < BUCKETS; ++b)
+    if (size_log2 < 0 || b == size_log2) row[b] = Choice{shape, ctas_per_sm};
   return SLEEK_OK;
 }
 
@@ -442,15 +533,18 @@ int sleek_workspace_status(const void* ws, void* stream, int* status)
       *status = SLEEK_OK;
       return SLEEK_OK;
     }
-    p = it->second.first;
+    p = it->second.ptr;
   }
-  unsigned long long v = 0;
+  unsigned long long h[HDR_WORDS];
   if (cudaStreamSynchronize(st) != cudaSuccess ||
-      cudaMemcpy(&v, static_cast<const unsigned long long*>(p) + 2, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaMemcpy(h, p, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
     cudaGetLastError();
     return SLEEK_ERR_CUDA;
   }
-  *status = static_cast<int>(v);
+  // the last single-buffer launch worked in the counter block of parity epoch - 1;
+  // batched runs (epoch 0) in block 0
+  const unsigned long long e = h[WS_EPOCH];
+  *status = static_cast<int>(h[(e ? ((e - 1) & 1) : 0) * WS_BLOCK + WS_STATUS]);
   return SLEEK_OK;
 }
 

@@ -22,8 +22,19 @@ constexpr unsigned ST_CORRUPT = 5;
 constexpr unsigned ST_TIMEOUT = 6;
 constexpr unsigned ST_CAPACITY = 9;
 
-// workspace header words (u64 each), followed by the look-back flag array
-enum WsWord { WS_TICKET = 0, WS_DONE = 1, WS_STATUS = 2, WS_TOTAL = 3, WS_ERRPOS = 4, WS_HDR_WORDS = 32 };
+// Workspace: 32 header words (u64 each), then the look-back flags.  The header
+// holds two blocks of per-launch counters (words 0-7 and 8-15), the launch epoch
+// (word 16) and words the range reduction uses (24-26).  Single-buffer launches
+// alternate between the blocks and between two flag regions by epoch parity (see
+// WsPhase below); batched launches use block 0 and the first region of a
+// workspace cleared before each run.
+enum WsWord {
+  WS_TICKET = 0, WS_DONE = 1, WS_STATUS = 2, WS_TOTAL = 3, WS_ERRPOS = 4, WS_USED = 5,  // within a block
+  WS_BLOCK = 8,       // words per counter block
+  WS_EPOCH = 16,      // launches completed on this workspace
+  WS_MINMAX = 24,     // three words for the range reduction (cleared by its own call)
+  WS_HDR_WORDS = 32
+};
 
 // look-back flag: state in bits 62-63, value in bits 0-61
 constexpr uint64_t FLAG_AGG = 1ull << 62;
@@ -152,13 +163,78 @@ __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p)
   return v;
 }
 
-// records the first error; later errors keep the first code
-__device__ __forceinline__ void set_status(uint64_t* ws, unsigned code, long long pos)
+// records the first error in a counter block; later errors keep the first code
+__device__ __forceinline__ void set_status(uint64_t* hdr, unsigned code, long long pos)
 {
-  if (atomicCAS(reinterpret_cast<unsigned long long*>(&ws[WS_STATUS]), 0ull, (unsigned long long)code) == 0ull) {
-    atomicExch(reinterpret_cast<unsigned long long*>(&ws[WS_ERRPOS]), (unsigned long long)pos);
+  if (atomicCAS(reinterpret_cast<unsigned long long*>(&hdr[WS_STATUS]), 0ull, (unsigned long long)code) == 0ull) {
+    atomicExch(reinterpret_cast<unsigned long long*>(&hdr[WS_ERRPOS]), (unsigned long long)pos);
   }
 }
+
+// ----------------------------------------------------------------------------
+// Self-resetting workspace of the single-buffer kernels.  A launch works in
+// counter block and flag region p = epoch & 1 (both clean when it starts), and
+// leaves the other parity clean for the next launch: every CTA clears its share
+// of the flags the previous launch used there, and the last CTA resets that
+// counter block, records how many flags this launch used, then advances the
+// epoch.  A workspace that starts zeroed therefore needs no clearing between
+// launches on one stream; a workspace cleared before every launch (epoch 0)
+// behaves the same.  flag_cap is the size of one flag region.
+// ----------------------------------------------------------------------------
+struct WsPhase {
+  uint64_t* hdr;        // this launch's counter block
+  uint64_t* hdr_other;  // the other block (the previous launch's)
+  uint64_t* flags;      // this launch's flag region
+  uint64_t* flags_other;
+  uint64_t epoch;
+  long long used_other;  // flags the previous launch left in the other region
+
+  __device__ static WsPhase of(uint64_t* ws, long long flag_cap)
+  {
+    WsPhase w;
+    w.epoch = ld_relaxed_u64(&ws[WS_EPOCH]);
+    const int p = static_cast<int>(w.epoch & 1u);
+    w.hdr = ws + WS_BLOCK * p;
+    w.hdr_other = ws + WS_BLOCK * (1 - p);
+    w.flags = ws + WS_HDR_WORDS + flag_cap * p;
+    w.flags_other = ws + WS_HDR_WORDS + flag_cap * (1 - p);
+    w.used_other = static_cast<long long>(ld_relaxed_u64(&w.hdr_other[WS_USED]));
+    return w;
+  }
+
+  // block 0 and the first flag region, nothing to clear (a workspace cleared
+  // before each launch, as the batched launches use it)
+  __device__ static WsPhase fixed(uint64_t* ws)
+  {
+    WsPhase w;
+    w.epoch = 0;
+    w.hdr = ws;
+    w.hdr_other = ws + WS_BLOCK;
+    w.flags = ws + WS_HDR_WORDS;
+    w.flags_other = w.flags;
+    w.used_other = 0;
+    return w;
+  }
+
+  // this CTA's share of the other region's flags, by the calling warp
+  __device__ void clear_other_share(int lane) const
+  {
+    const long long per = (used_other + gridDim.x - 1) / gridDim.x;
+    const long long b = per * blockIdx.x;
+    const long long e = min(b + per, used_other);
+    for (long long i = b + lane; i < e; i += 32) flags_other[i] = 0ull;
+  }
+
+  // the last CTA, one thread, after every CTA has counted itself done
+  __device__ void finish(uint64_t* ws, long long used) const
+  {
+    hdr[WS_USED] = static_cast<uint64_t>(used);
+#pragma unroll
+    for (int i = 0; i < WS_BLOCK; ++i) hdr_other[i] = 0ull;
+    __threadfence();
+    ws[WS_EPOCH] = epoch + 1u;
+  }
+};
 
 // ----------------------------------------------------------------------------
 // value transforms (restated from include/sleek_common_gpu.h of the reference:
@@ -453,10 +529,6 @@ __device__ __forceinline__ long long warp_sum(long long v)
   return v;
 }
 
-// padded index of value k in the transformed-value buffer (one pad slot per 32
-// values keeps the gather reads of the packer on distinct banks)
-__device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
-
 // ----------------------------------------------------------------------------
 // Decoupled look-back over flag words.  Called by one whole warp for item
 // `idx` whose segment starts at `seg_begin` (items before the segment count as
@@ -465,10 +537,10 @@ __device__ __forceinline__ int tpad(int k) { return k + (k >> 5); }
 // nearest inclusive prefix, and slides past runs of aggregates; it only waits
 // when the nearest unresolved flag is not published yet.  Returns the exclusive
 // prefix, or -1 when a wait exceeded `limit_ns` or another CTA already
-// reported an error.
+// reported an error in the counter block `hdr`.
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ long long lookback(const uint64_t* flags, long long idx, long long seg_begin,
-                                              const uint64_t* ws, unsigned long long limit_ns = SPIN_TIMEOUT_NS)
+                                              const uint64_t* hdr, unsigned long long limit_ns = SPIN_TIMEOUT_NS)
 {
   constexpr int PER = 1;  // polls of 32 flags: measured against 64 and 128, encode +2 % and +4-9 %
   const int lane = threadIdx.x & 31;
@@ -514,7 +586,7 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
       t0 = globaltimer_ns();
     } else if (polls > 64 && (polls & 63) == 0) {
       const bool late = globaltimer_ns() - t0 > limit_ns;
-      const bool failed = ld_relaxed_u64(&ws[WS_STATUS]) != 0ull;
+      const bool failed = ld_relaxed_u64(&hdr[WS_STATUS]) != 0ull;
       if (__any_sync(0xffffffffu, late || failed)) return -1;
     }
     // sleeping from the first miss keeps hundreds of waiting warps from flooding
@@ -525,11 +597,12 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
 }
 
 // ----------------------------------------------------------------------------
-// Shifted store: writes `len` bytes from 16-byte aligned shared memory `src`
-// to the arbitrary global byte address `dst`.  Whole aligned 16-byte granules
-// get one vector store each, funnel-shifted from two aligned shared loads; the
-// at most two granules shared with neighbouring chunks are written byte by
-// byte.  Called by all NT threads.
+// Shifted store by one warp: writes `len` bytes from 16-byte aligned shared
+// memory `src` to the arbitrary global byte address `dst`.  The whole aligned
+// 16-byte granules go out in 32-byte aligned pairs, one 256-bit store each,
+// funnel-shifted from three aligned shared loads, consecutive lanes on
+// consecutive pairs (a warp instruction fills whole lines); the at most two
+// granules shared with neighbouring chunks are written byte by byte.
 // ----------------------------------------------------------------------------
 template <int WQ>
 __device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, int bb8)
@@ -544,63 +617,81 @@ __device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, i
   return o;
 }
 
-// Granules jf .. jl-1, consecutive lanes on consecutive granules (so a warp's
-// loads hit every bank once and its stores fill whole sectors), two granules in
-// flight per thread.
-template <int WQ, int NT>
-__device__ __forceinline__ void shifted_run(uint4* out, const uint4* s4, int jf, int jl, int bb8)
+// 32-byte global store (sm_100: one 256-bit access); p must be 32-byte aligned
+__device__ __forceinline__ void st_global_v8(void* p, const uint4 a, const uint4 b)
 {
-  for (int j = jf + static_cast<int>(threadIdx.x); j < jl; j += 2 * NT) {
-    const bool two = j + NT < jl;
-    const uint4 x0 = s4[j - 1], y0 = s4[j];
-    uint4 x1 = x0, y1 = y0;
-    if (two) {
-      x1 = s4[j + NT - 1];
-      y1 = s4[j + NT];
-    }
-    out[j] = shifted_granule<WQ>(x0, y0, bb8);
-    if (two) out[j + NT] = shifted_granule<WQ>(x1, y1, bb8);
-  }
+  asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+               "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+               : "memory");
 }
 
-template <int NT>
-__device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len)
+// Output granule j of a run shifted by WQ words and bb8 bits (WQ < 0: no shift).
+template <int WQ>
+__device__ __forceinline__ uint4 out_granule(const uint4* s4, int j, int bb8)
 {
-  const int tid = threadIdx.x;
+  if constexpr (WQ < 0) return s4[j];
+  else return shifted_granule<WQ>(s4[j - 1], s4[j], bb8);
+}
+
+// Granules jf .. jl-1 of the output: 32-byte aligned pairs, one per lane and
+// iteration (consecutive lanes on consecutive pairs), each from three aligned
+// shared loads; the at most two unpaired granules by lanes 0 and 1.
+template <int WQ>
+__device__ __forceinline__ void shifted_pairs_warp(uint4* out, const uint4* s4, int jf, int jl, int bb8, int par,
+                                                   int lane)
+{
+  const int jp = jf + ((jf + par) & 1);  // first granule that starts a 32-byte aligned pair
+  const int np = jl - jp >= 0 ? (jl - jp) >> 1 : 0;
+  for (int k = lane; k < np; k += 32) {
+    const int j = jp + 2 * k;
+    if constexpr (WQ < 0) {
+      st_global_v8(out + j, s4[j], s4[j + 1]);
+    } else {
+      const uint4 x = s4[j - 1], y = s4[j], z = s4[j + 1];
+      st_global_v8(out + j, shifted_granule<WQ>(x, y, bb8), shifted_granule<WQ>(y, z, bb8));
+    }
+  }
+  int j = -1;
+  if (lane == 0 && jp > jf && jf < jl) j = jf;
+  if (lane == 1 && jp + 2 * np < jl) j = jp + 2 * np;
+  if (j >= 0) out[j] = out_granule<WQ>(s4, j, bb8);
+}
+
+__device__ __forceinline__ void store_shifted_warp(uint8_t* dst, const uint8_t* src, int len, int lane)
+{
   const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
   const int sft = static_cast<int>(d & 15u);
   uint8_t* const a0 = dst - sft;
+  const int par = static_cast<int>((reinterpret_cast<uintptr_t>(a0) >> 4) & 1u);
   uint4* const out = reinterpret_cast<uint4*>(a0);
   const uint4* const s4 = reinterpret_cast<const uint4*>(src);
   const int nunits = (sft + len + 15) >> 4;
   const int jf = sft ? 1 : 0;              // first granule entirely inside the chunk
   const int jl = (sft + len) >> 4;         // one past the last such granule
   if (sft == 0) {
-    for (int j = tid; j < jl; j += NT) out[j] = s4[j];
+    shifted_pairs_warp<-1>(out, s4, jf, jl, 0, par, lane);
   } else {
     const int bo = 16 - sft;
     const int bb8 = (bo & 3) * 8;
     switch (bo >> 2) {
-      case 0: shifted_run<0, NT>(out, s4, jf, jl, bb8); break;
-      case 1: shifted_run<1, NT>(out, s4, jf, jl, bb8); break;
-      case 2: shifted_run<2, NT>(out, s4, jf, jl, bb8); break;
-      default: shifted_run<3, NT>(out, s4, jf, jl, bb8); break;
+      case 0: shifted_pairs_warp<0>(out, s4, jf, jl, bb8, par, lane); break;
+      case 1: shifted_pairs_warp<1>(out, s4, jf, jl, bb8, par, lane); break;
+      case 2: shifted_pairs_warp<2>(out, s4, jf, jl, bb8, par, lane); break;
+      default: shifted_pairs_warp<3>(out, s4, jf, jl, bb8, par, lane); break;
     }
   }
-  // edge granules (shared with the neighbouring chunks): one byte per lane of
-  // the first warp, lanes 0-15 the first granule, lanes 16-31 the last
-  if (tid < 32) {
-    int e = -1;
-    if (tid < 16) {
-      if (sft != 0) e = 0;
-    } else {
-      const int last = nunits - 1;
-      if (last >= jl && !(last == 0 && sft != 0)) e = last;
-    }
-    if (e >= 0) {
-      const int r = 16 * e - sft + (tid & 15);  // source byte of this lane
-      if (r >= 0 && r < len) a0[16 * e + (tid & 15)] = src[r];
-    }
+  // edge granules (shared with the neighbouring chunks): one byte per lane,
+  // lanes 0-15 the first granule, lanes 16-31 the last
+  int e = -1;
+  if (lane < 16) {
+    if (sft != 0) e = 0;
+  } else {
+    const int last = nunits - 1;
+    if (last >= jl && !(last == 0 && sft != 0)) e = last;
+  }
+  if (e >= 0) {
+    const int r = 16 * e - sft + (lane & 15);  // source byte of this lane
+    if (r >= 0 && r < len) a0[16 * e + (lane & 15)] = src[r];
   }
 }
 

@@ -27,17 +27,30 @@
 
 namespace sleek {
 
-constexpr int ENC_STAGES = 4;
-constexpr int ENC_LAG = ENC_STAGES - 2;  // chunks computed but not yet stored
-// the stage freed by storing chunk k - ENC_LAG (end of iteration k) takes chunk
-// k + ENC_AHEAD: the producer runs ENC_AHEAD - 1 chunks ahead of the compute warps
-constexpr int ENC_AHEAD = ENC_STAGES - ENC_LAG;
-constexpr int ENC_CW = 8;                    // compute warps
-constexpr int ENC_NT = (ENC_CW + 2) * 32;    // + a producer warp and a scanner warp
-constexpr int ENC_MINB = 3;
+// Launch shape of the encode kernel: CW compute warps (each takes SC / CW
+// subchunks of a chunk), ST shared-memory stages of one chunk each, and a
+// producer that takes chunk k's ticket and issues its copy once the compute warps
+// have begun chunk k - AHEAD (and the stage's previous chunk is stored), so
+// tickets are taken at most AHEAD chunks ahead of the compute warps.  MINB is the
+// CTAs per SM the registers are budgeted for.  Every shape writes the same bytes.
+template <int CW_, int ST_, int AHEAD_, int MINB_>
+struct EncShape {
+  static constexpr int CW = CW_;
+  static constexpr int ST = ST_;
+  static constexpr int AHEAD = AHEAD_;
+  static constexpr int MINB = MINB_;
+  static constexpr int NT = (CW + 2) * 32;  // + a producer warp and a placer warp
+  static constexpr int SPW = SC / CW;       // subchunks per compute warp
+  static_assert(SC % CW == 0 && AHEAD >= 1 && AHEAD < ST, "shape");
+};
+// the shapes the library is built with (index = the C ABI's shape number)
+using EncShape0 = EncShape<8, 4, 2, 3>;   // default: 10 warps, 66 KB, 3 CTAs per SM
+using EncShape1 = EncShape<16, 4, 2, 2>;  // 18 warps, 66 KB, 2 CTAs per SM
+using EncShape2 = EncShape<4, 4, 2, 3>;   // 6 warps, 66 KB, 3 CTAs per SM
+constexpr int ENC_SHAPES = 3;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
-// What the producer tells the compute and scanner warps about the chunk in a stage.
+// What the producer tells the compute and placer warps about the chunk in a stage.
 struct EncMeta {
   long long g;          // look-back flag index (chunk id across the launch), or NO_CHUNK
   long long c;          // chunk index within its buffer
@@ -46,7 +59,7 @@ struct EncMeta {
   long long insize;     // bytes of the buffer
   uint8_t* out;         // the buffer's stream
   long long* outsize;   // the buffer's size output
-  long long excl;       // payload offset of the chunk (scanner), -1 after an error
+  long long excl;       // payload offset of the chunk (placer), -1 after an error
   QParams q;            // the buffer's quantizer parameters
   int kind;             // bit 0: 64-bit values, bit 1: lossy
   int osize;
@@ -54,19 +67,30 @@ struct EncMeta {
   int comp;
 };
 
+template <int ST>
 struct EncMisc {
-  uint64_t full[ENC_STAGES];    // chunk bytes landed (TMA tx count)
-  uint64_t empty[ENC_STAGES];   // go-ahead for the stage's next copy (its previous chunk is stored)
-  uint64_t sized[ENC_STAGES];   // compressed size of the stage's chunk known
-  uint64_t placed[ENC_STAGES];  // payload offset of the stage's chunk known
-  EncMeta meta[ENC_STAGES];
+  uint64_t full[ST];    // chunk bytes landed (TMA tx count)
+  uint64_t empty[ST];   // the stage's chunk is stored (placer): the stage may be refilled
+  uint64_t began[ST];   // the compute warps are past phase A of the stage's chunk
+  uint64_t sized[ST];   // compressed size of the stage's chunk known
+  uint64_t packed[ST];  // every compute warp has packed its share of the stage's chunk
+  EncMeta meta[ST];
   int lnv[2][SC];  // subchunk bit widths, by chunk parity (a fast warp may write the next chunk's)
 };
 
-constexpr int ENC_SMEM = ENC_STAGES * STAGE_BYTES + ((sizeof(EncMisc) + 127) / 128) * 128;
-constexpr int ENC_BATCH_SMEM = ENC_SMEM + 8 * (BATCH_MAX_JOBS + 1);  // + the jobs' first chunk ids
+template <class S>
+constexpr int enc_smem()
+{
+  return S::ST * STAGE_BYTES + static_cast<int>((sizeof(EncMisc<S::ST>) + 127) / 128) * 128;
+}
+template <class S>
+constexpr int enc_batch_smem()
+{
+  return enc_smem<S>() + 8 * (BATCH_MAX_JOBS + 1);  // + the jobs' first chunk ids
+}
 
-// barrier among the compute warps only (named barrier 1), OR-reducing `pred`
+// barrier among the CW compute warps only (named barrier 1), OR-reducing `pred`
+template <int CW>
 __device__ __forceinline__ bool cbar_or(bool pred)
 {
   uint32_t r;
@@ -76,7 +100,7 @@ __device__ __forceinline__ bool cbar_or(bool pred)
       "bar.red.or.pred q, 1, %2, p;\n\t"
       "selp.u32 %0, 1, 0, q;\n\t}"
       : "=r"(r)
-      : "r"(static_cast<uint32_t>(pred)), "n"(ENC_CW * 32)
+      : "r"(static_cast<uint32_t>(pred)), "n"(CW * 32)
       : "memory");
   return r != 0;
 }
@@ -205,8 +229,9 @@ __device__ __forceinline__ void run_words(const uint32_t (&v)[4], int ln, uint32
 
 // Packs a warp's SPW subchunks (offsets wbase, widths lnu).  When every run is
 // short, or (32-bit values) every run is long (32 <= P*ln, ln below the value
-// width), the subchunks go through one straight-line sequence each, so their
-// shuffles, shifts and stores overlap; other widths take the per-subchunk path.
+// width), or (64-bit values) every run is long with values of at most 31 bits,
+// the subchunks go through one straight-line sequence each, so their shuffles,
+// shifts and stores overlap; other widths take the per-subchunk path.
 // (For 64-bit values the branch-free long run costs more than the overlap saves:
 // measured -2 % on lossless f64, +3.5-6 % on f32.)
 constexpr int PACK_GROUP = 2;  // subchunks whose long runs are built and exchanged together
@@ -217,11 +242,12 @@ __device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[
 {
   constexpr int P = 16 / static_cast<int>(sizeof(T));
   constexpr int TB = 8 * static_cast<int>(sizeof(T));
-  bool all_long = sizeof(T) == 4, all_short = true;
+  bool all_long = sizeof(T) == 4, all_short = true, all_narrow = sizeof(T) == 8;
 #pragma unroll
   for (int u = 0; u < SPW; ++u) {
     all_long &= P * lnu[u] >= 32 && lnu[u] < TB;
     all_short &= P * lnu[u] < 32;
+    all_narrow &= P * lnu[u] >= 32 && lnu[u] < 32;  // 64-bit values of 16 .. 31 bits
   }
   if (all_long) {
     if constexpr (sizeof(T) == 4) {
@@ -281,6 +307,36 @@ __device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[
       if (!first[u] && lo[u]) atomicOr(&pw[w[u]], lo[u]);
       if (hi[u]) atomicOr(&pw[w[u] + 1], hi[u]);
     }
+  } else if (all_narrow) {
+    if constexpr (sizeof(T) == 8) {
+      // 64-bit values that fit in 31 bits (typical of lossy chunks): the lane's two
+      // values make a run of 32 .. 62 bits, two words before the shift and at most
+      // three after it, built from the low halves only
+      uint32_t y0[SPW], y1[SPW], tl[SPW], pv[SPW];
+      int nf[SPW];
+#pragma unroll
+      for (int u = 0; u < SPW; ++u) {
+        const int ln = lnu[u];
+        const int R = P * ln;
+        const int sh = (lane * R) & 31;
+        const uint32_t a0 = static_cast<uint32_t>(v[u][0]), b0 = static_cast<uint32_t>(v[u][1]);
+        const uint32_t x0 = a0 | (b0 << ln), x1 = __funnelshift_l(b0, 0u, ln);
+        y0[u] = x0 << sh;
+        y1[u] = __funnelshift_l(x0, x1, sh);
+        const uint32_t y2 = __funnelshift_l(x1, 0u, sh);
+        nf[u] = (sh + R) >> 5;
+        tl[u] = nf[u] == 1 ? y1[u] : y2;
+      }
+#pragma unroll
+      for (int u = 0; u < SPW; ++u) pv[u] = __shfl_up_sync(0xffffffffu, tl[u], 1);
+#pragma unroll
+      for (int u = 0; u < SPW; ++u) {
+        const int rs = lane * P * lnu[u];
+        uint32_t* const d = pw + wbase[u] + (rs >> 5);
+        d[0] = (rs & 31) ? (y0[u] | pv[u]) : y0[u];
+        if (nf[u] > 1) d[1] = y1[u];
+      }
+    }
   } else {
 #pragma unroll
     for (int u = 0; u < SPW; ++u) pack_subchunk<T>(pw + wbase[u], lnu[u], v[u], lane);
@@ -294,15 +350,15 @@ __device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[
 // there, with `skip` (no chunk: the end, or a failed wait) and `fail` (this
 // thread's wait gave up); returns 2 if any thread failed, 1 at the end, 0 when
 // the chunk was processed.
-template <int KIND>
-__device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc& m, uint64_t* flags, int cw,
+template <int KIND, class S>
+__device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc<S::ST>& m, uint64_t* flags, int cw,
                                              int lane, int tid, int par, bool skip, bool fail)
 {
   using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
   constexpr bool LOSSY = (KIND & 2) != 0;
   using V = VT<T>;
   constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane per subchunk
-  constexpr int SPW = SC / ENC_CW;                      // subchunks per compute warp
+  constexpr int SPW = S::SPW;                            // subchunks per compute warp
   int* const lnv = m.lnv[par];
 
   // ---- phase A: values into registers, transform / quantize, bit widths ------
@@ -312,7 +368,7 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
   const QParams q = me.q;
 #pragma unroll
   for (int u = 0; u < SPW; ++u) {
-    const int i = cw + u * ENC_CW;
+    const int i = cw + u * S::CW;
     const uint4 w4 = *reinterpret_cast<const uint4*>(stg + i * 512 + lane * 16);
     if constexpr (sizeof(T) == 4) {
       vals[u][0] = w4.x; vals[u][1] = w4.y; vals[u][2] = w4.z; vals[u][3] = w4.w;
@@ -330,7 +386,7 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
     if (lane == 0) lnv[i] = w;
   }
   }
-  if (cbar_or(fail)) return 2;
+  if (cbar_or<S::CW>(fail)) return 2;
   if (skip) return 1;
 
   // ---- widths scan (every warp, redundantly), size decision -----------------
@@ -343,10 +399,12 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
   const bool comp = newsize < osize;
   const int csize = comp ? newsize : osize;
   if (tid == 0) {
+    const int s = static_cast<int>(&me - m.meta);
     me.csize = csize;
     me.comp = comp;
     st_relaxed_u64(&flags[me.g], (me.c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
-    mbar_arrive(&m.sized[&me - m.meta]);
+    mbar_arrive(&m.sized[s]);
+    mbar_arrive(&m.began[s]);
   }
 
   // ---- pack this chunk from registers ----------------------------------------
@@ -355,7 +413,7 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc&
     int wbase[SPW], lnu[SPW];  // all offsets and widths first: the reductions overlap
 #pragma unroll
     for (int u = 0; u < SPW; ++u) {
-      const int i = cw + u * ENC_CW;
+      const int i = cw + u * S::CW;
       wbase[u] = __reduce_add_sync(0xffffffffu, lane < i ? wc : 0);  // words of subchunks before i
       lnu[u] = __shfl_sync(0xffffffffu, ln_l, i);
     }
@@ -424,19 +482,30 @@ struct EncSource<true> {
   }
 };
 
-template <int KIND, bool BATCH, int MINB>
-__global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::conditional<BATCH, BatchEncArgs, EncArgs>::type a)
+template <int KIND, bool BATCH, class S>
+__global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::conditional<BATCH, BatchEncArgs, EncArgs>::type a)
 {
+  constexpr int ENC_STAGES = S::ST;
+  constexpr int ENC_AHEAD = S::AHEAD;
+  constexpr int ENC_CW = S::CW;
+  constexpr int ENC_NT = S::NT;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* const stage0 = smem;
-  EncMisc& m = *reinterpret_cast<EncMisc*>(smem + ENC_STAGES * STAGE_BYTES);
-  long long* const cb = reinterpret_cast<long long*>(smem + ENC_SMEM);
+  EncMisc<ENC_STAGES>& m = *reinterpret_cast<EncMisc<ENC_STAGES>*>(smem + ENC_STAGES * STAGE_BYTES);
+  long long* const cb = reinterpret_cast<long long*>(smem + enc_smem<S>());
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  uint64_t* const ws = a.ws;
-  uint64_t* const flags = ws + WS_HDR_WORDS;
+  // this launch's counter block and flag region: alternating by epoch in the
+  // single-buffer form (self-resetting workspace), block 0 and the first region
+  // of a workspace cleared before each run in the batched form
+  const WsPhase ph = [&]() {
+    if constexpr (BATCH) return WsPhase::fixed(a.ws);
+    else return WsPhase::of(a.ws, a.flag_cap);
+  }();
+  uint64_t* const hdr = ph.hdr;
+  uint64_t* const flags = ph.flags;
 
   if constexpr (BATCH) {
     for (int i = tid; i <= a.njobs; i += ENC_NT) cb[i] = a.chunk_base[i];
@@ -444,9 +513,10 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
   if (tid == 0) {
     for (int s = 0; s < ENC_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
-      mbar_init(&m.empty[s], ENC_CW);  // one arrival per compute warp
+      mbar_init(&m.empty[s], 1);
+      mbar_init(&m.began[s], 1);
       mbar_init(&m.sized[s], 1);
-      mbar_init(&m.placed[s], 1);
+      mbar_init(&m.packed[s], ENC_CW);  // one arrival per compute warp
     }
     mbar_fence_init();
   }
@@ -463,21 +533,22 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
     // look-back wait for it.
-    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]);
+    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&hdr[WS_TICKET]);
     unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
     unsigned issued_par = 0;  // parity of that use
     bool more = true;
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      // From seq ENC_AHEAD on, the copy for chunk seq is issued once every compute
-      // warp has finished chunk seq - ENC_AHEAD, in which the stage's previous
-      // chunk, seq - ENC_STAGES, was stored.
-      if (seq >= ENC_AHEAD) {
-        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
-        if (__any_sync(0xffffffffu, !ok)) {
-          if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
-          break;
-        }
+      // The copy for chunk seq is issued once the compute warps are past phase A
+      // of chunk seq - ENC_AHEAD and the placer has stored the stage's previous
+      // chunk, seq - ENC_STAGES.
+      bool ok = true;
+      if (seq >= ENC_AHEAD)
+        ok = mbar_wait_bounded(&m.began[(seq - ENC_AHEAD) % ENC_STAGES], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
+      if (ok && seq >= ENC_STAGES) ok = mbar_wait_bounded(&m.empty[s], ((seq / ENC_STAGES) - 1) & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+        break;
       }
       long long t = NO_CHUNK;
       if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
@@ -536,7 +607,10 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
         if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
   } else if (warp == ENC_CW + 1) {
-    // ===================== scanner warp: decoupled look-back =====================
+    // ============ placer warp: decoupled look-back, then the chunk's store ============
+    // The compute warps never wait for a chunk's offset: they pack it and move on,
+    // and this warp places it once its look-back is done.
+    if constexpr (!BATCH) ph.clear_other_share(lane);
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
       const uint32_t par = (seq / ENC_STAGES) & 1;
@@ -552,75 +626,59 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       unsigned err = 0;
       ok = mbar_wait_bounded(&m.sized[s], par);
       if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, g);
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, g);
         break;
       }
       if (c > 0) {
-        excl = lookback(flags, g, me.seg, ws);
+        excl = lookback(flags, g, me.seg, hdr);
         if (excl < 0) err = ST_TIMEOUT;
         else if (excl > c * CS) err = ST_CAPACITY;
         if (err) excl = -1;
       }
       const int csize = me.csize;
-      if (c > 0) {
-        if (lane == 0) {
-          if (err) set_status(ws, err, g);
+      uint8_t* const out = me.out;
+      if (lane == 0) {
+        if (c > 0) {
+          if (err) set_status(hdr, err, g);
           // an impossible prefix is replaced by the largest legal one so that
           // every later chunk still writes inside the output bound
           st_relaxed_u64(&flags[g], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
         }
-      }
-      if (lane == 0) {
-        me.excl = excl;
         if (c == me.chunks - 1 && excl >= 0) {
           if constexpr (BATCH) {  // the buffer is complete: its header and size
-            *reinterpret_cast<long long*>(me.out) = me.insize;
+            *reinterpret_cast<long long*>(out) = me.insize;
             *me.outsize = 8 + 2 * me.chunks + excl + csize;
           } else {
-            ws[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
+            hdr[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
           }
         }
-        mbar_arrive(&m.placed[s]);
       }
+      // the compute warps' packed bytes (or the raw chunk) are complete in the stage
+      ok = mbar_wait_bounded(&m.packed[s], par);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, g);
+        break;
+      }
+      if (excl >= 0) {
+        store_shifted_warp(out + 8 + 2 * me.chunks + excl, stage0 + s * STAGE_BYTES, csize, lane);
+        if (lane == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
+      }
+      // the producer may refill the stage (generic reads ordered before its TMA write)
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&m.empty[s]);
     }
   } else {
     // ===================== compute warps =====================
-    const int cw = warp;
-    auto store = [&](int sq) {  // all compute threads; placed[] already observed
-      const int sp = sq % ENC_STAGES;
-      const EncMeta& me = m.meta[sp];
-      const long long excl = me.excl;
-      if (excl >= 0) {
-        uint8_t* const out = me.out;
-        const long long c = me.c;
-        const int csize = me.csize;
-        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize);
-        if (tid == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
-      }
-    };
-
-    // Each thread waits for the offset itself; a wait that gives up skips this
-    // thread's share of the store and is reported at the next barrier.
-    auto placed_store = [&](int sq) -> bool {
-      if (!mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1)) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
-        return false;
-      }
-      store(sq);
-      return true;
-    };
-
     // Warps pass each other freely between the barriers of compute_chunk: each
-    // waits for its stage and its offsets itself and frees a stage with its own
-    // arrival, and the pack data one warp stores were written by the others
-    // before an earlier barrier.
-    int seq = 0;
-    bool failed = false;
+    // waits for its stage itself and reports its share of a chunk packed with its
+    // own arrival; the placer stores the chunk once every warp has.
+    const int cw = warp;
     bool late = false;  // a wait of this thread gave up
-    for (;; ++seq) {
+    for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
       if (!mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1)) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, -1);
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
         late = true;
       }
       EncMeta& me = m.meta[s];
@@ -630,34 +688,19 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
       int r;
       if constexpr (KIND >= 0) {
-        r = compute_chunk<KIND>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate);
+        r = compute_chunk<KIND, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate);
       } else {
         switch (skip ? 0 : me.kind) {
-          case 0: r = compute_chunk<0>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
-          case 1: r = compute_chunk<1>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
-          case 2: r = compute_chunk<2>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
-          default: r = compute_chunk<3>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          case 0: r = compute_chunk<0, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          case 1: r = compute_chunk<1, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          case 2: r = compute_chunk<2, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
+          default: r = compute_chunk<3, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
         }
       }
-      if (r == 2) {
-        failed = true;
-        break;
-      }
-      if (r == 1) break;
-      // ---- store the chunk of seq - ENC_LAG once its offset is known -----------
-      // (waiting here rather than before the compute gives its look-back one
-      // more chunk of compute time to finish)
-      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) late = true;
-      // this warp is done with the stage of seq - ENC_LAG, which the producer may
-      // now refill with chunk seq + ENC_AHEAD (generic accesses ordered before its TMA write)
-      fence_proxy_async_smem();
+      if (r != 0) break;  // the end, or a wait that gave up (reported)
+      // this warp's share of the chunk is packed (its shared stores before the arrival)
       __syncwarp();
-      if (lane == 0) mbar_arrive(&m.empty[(seq + ENC_AHEAD) % ENC_STAGES]);
-    }
-    if (!failed) {
-      // drain: chunks seq - ENC_LAG .. seq - 1
-      for (int q = seq >= ENC_LAG ? seq - ENC_LAG : 0; q < seq; ++q)
-        if (!placed_store(q)) break;
+      if (lane == 0) mbar_arrive(&m.packed[s]);
     }
   }
 
@@ -666,13 +709,13 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
   __shared__ int last_cta;
   if (tid == 0) {
     __threadfence();
-    const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
+    const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_DONE]), 1ull);
     last_cta = d == gridDim.x - 1;
     if (last_cta) __threadfence();
   }
   __syncthreads();
   if (last_cta) {
-    const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+    const unsigned long long st = ld_relaxed_u64(&hdr[WS_STATUS]);
     if constexpr (BATCH) {
       // buffers without chunks get their header-only stream; an error anywhere
       // turns every size into -status
@@ -687,9 +730,10 @@ __global__ void __launch_bounds__(ENC_NT, MINB) k_encode(const typename std::con
       }
     } else if (tid == 0) {
       const long long chunks = (a.insize + CS - 1) / CS;
-      const long long tot = chunks ? static_cast<long long>(ld_relaxed_u64(&ws[WS_TOTAL])) : 0ll;
+      const long long tot = chunks ? static_cast<long long>(ld_relaxed_u64(&hdr[WS_TOTAL])) : 0ll;
       *reinterpret_cast<long long*>(a.out) = a.insize;
       *a.outsize = st ? -static_cast<long long>(st) : 8 + 2 * chunks + tot;
+      ph.finish(a.ws, chunks);
     }
   }
 }
@@ -812,8 +856,9 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  uint64_t* const ws = a.ws;
-  uint64_t* const flags = ws + WS_HDR_WORDS;
+  const WsPhase ph = WsPhase::of(a.ws, a.flag_cap);  // self-resetting workspace
+  uint64_t* const hdr = ph.hdr;
+  uint64_t* const flags = ph.flags;
 
   // header checks (every CTA reads the 8-byte header)
   const long long insize = *reinterpret_cast<const long long*>(a.in);
@@ -831,9 +876,9 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       mbar_init(&m.empty[st], NW);  // one arrival per warp
     }
     mbar_fence_init();
-    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_TICKET]), 1ull));
-    if (!hdr_ok) set_status(ws, ST_CORRUPT, -1);
-    else if (!cap_ok) set_status(ws, ST_CAPACITY, -1);
+    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_TICKET]), 1ull));
+    if (!hdr_ok) set_status(hdr, ST_CORRUPT, -1);
+    else if (!cap_ok) set_status(hdr, ST_CAPACITY, -1);
   }
   __syncthreads();
 
@@ -865,13 +910,13 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       int b2 = lane < NW ? m.bad[lane] : 0;
       s2 = warp_sum(s2);
       b2 = __any_sync(0xffffffffu, b2);
-      if (b2 && lane == 0) set_status(ws, ST_CORRUPT, c0);
+      if (b2 && lane == 0) set_status(hdr, ST_CORRUPT, c0);
       if (lane == 0) st_relaxed_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
       long long excl = 0;
       if (vb > 0) {
-        excl = lookback(flags, vb, 0, ws);
+        excl = lookback(flags, vb, 0, hdr);
         if (excl < 0) {
-          if (lane == 0) set_status(ws, ST_TIMEOUT, c0);
+          if (lane == 0) set_status(hdr, ST_TIMEOUT, c0);
         }
         if (lane == 0)
           st_relaxed_u64(&flags[vb], FLAG_INC | (static_cast<uint64_t>(excl >= 0 ? excl + s2 : 0) & FLAG_VAL));
@@ -936,7 +981,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       const int st = jt % DEC_STAGES;
       if (jt >= DEC_STAGES &&
           __any_sync(0xffffffffu, !mbar_wait_bounded(&m.empty[st], ((jt - DEC_STAGES) / DEC_STAGES) & 1))) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, issued);
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, issued);
         feeding = false;
         return;
       }
@@ -953,7 +998,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       if (warp == 0 && feeding && issued < c1) issue_next();
 
       if (__any_sync(0xffffffffu, !mbar_wait_bounded(&m.full[s], (it / DEC_STAGES) & 1))) {
-        if (lane == 0) set_status(ws, ST_TIMEOUT, c);
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, c);
         break;
       }
 
@@ -961,10 +1006,10 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       const int osize = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
       uint8_t* const outc = a.out + c * CS;
       if (!d.ok) {
-        if (tid == 0) set_status(ws, ST_CORRUPT, c);
+        if (tid == 0) set_status(hdr, ST_CORRUPT, c);
       } else if (!decode_chunk_warp<T, LOSSY, NW>(stg, d.sft, d.cs, osize, reinterpret_cast<T*>(outc), a.q,
                                                     warp, lane)) {
-        if (tid == 0) set_status(ws, ST_CORRUPT, c);
+        if (tid == 0) set_status(hdr, ST_CORRUPT, c);
       }
       // this warp is done with the stage (generic accesses ordered before the next TMA write)
       fence_proxy_async_smem();
@@ -985,11 +1030,12 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   __syncthreads();
   if (tid == 0) {
     __threadfence();
-    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&ws[WS_DONE]), 1ull);
+    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_DONE]), 1ull);
     if (dn == gridDim.x - 1) {
       __threadfence();
-      const unsigned long long st = ld_relaxed_u64(&ws[WS_STATUS]);
+      const unsigned long long st = ld_relaxed_u64(&hdr[WS_STATUS]);
       *a.outsize = st ? -static_cast<long long>(st) : insize;
+      ph.finish(a.ws, gridDim.x);
     }
   }
 }
@@ -1245,51 +1291,153 @@ static cudaError_t ensure_smem_attr(K k, int bytes, unsigned long long* done_mas
   return e;
 }
 
-template <typename T, bool LOSSY>
-static cudaError_t launch_encode_t(const EncArgs& a, int grid, cudaStream_t st)
+// Decode launch shapes: threads per CTA and the CTAs per SM the registers are
+// budgeted for (index = the C ABI's shape number).
+template <int NT_, int MINB_>
+struct DecShape {
+  static constexpr int NT = NT_;
+  static constexpr int MINB = MINB_;
+};
+using DecShape0 = DecShape<256, 4>;  // default
+using DecShape1 = DecShape<128, 6>;
+using DecShape2 = DecShape<512, 2>;
+constexpr int DEC_SHAPES = 3;
+
+template <int KIND, class S>
+static cudaError_t launch_enc_k(const EncArgs& a, int grid, cudaStream_t st)
 {
-  auto k = k_encode<(sizeof(T) == 8 ? 1 : 0) | (LOSSY ? 2 : 0), false, ENC_MINB>;
+  auto k = k_encode<KIND, false, S>;
   static unsigned long long attr = 0;
-  cudaError_t e = ensure_smem_attr(k, ENC_SMEM, &attr);
+  cudaError_t e = ensure_smem_attr(k, enc_smem<S>(), &attr);
   if (e != cudaSuccess) return e;
-  k<<<grid, ENC_NT, ENC_SMEM, st>>>(a);
+  k<<<grid, S::NT, enc_smem<S>(), st>>>(a);
   return cudaGetLastError();
 }
 
-template <typename T, bool LOSSY>
-static cudaError_t launch_decode_t(const DecArgs& a, int grid, cudaStream_t st)
+template <int KIND, class S>
+static int enc_occupancy()
 {
-  constexpr int NT = 256, MINB = 4;
-  auto k = k_decode<T, LOSSY, NT, MINB>;
-  static unsigned long long attr = 0;
-  cudaError_t e = ensure_smem_attr(k, DEC_SMEM, &attr);
-  if (e != cudaSuccess) return e;
-  k<<<grid, NT, DEC_SMEM, st>>>(a);
-  return cudaGetLastError();
-}
-
-template <typename T, bool LOSSY>
-static int occupancy_t(bool enc)
-{
+  auto k = k_encode<KIND, false, S>;
+  // the smem attribute must be set before the occupancy query counts dynamic smem
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, enc_smem<S>());
   int n = 0;
-  if (enc) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<(sizeof(T) == 8 ? 1 : 0) | (LOSSY ? 2 : 0), false, ENC_MINB>, ENC_NT, ENC_SMEM);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_decode<T, LOSSY, 256, 4>, 256, DEC_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, S::NT, enc_smem<S>());
   return n;
 }
 
-cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cudaStream_t st)
+template <typename T, bool LOSSY, class S>
+static cudaError_t launch_dec_k(const DecArgs& a, int grid, cudaStream_t st)
 {
-  if (width == 4) return lossy ? launch_encode_t<uint32_t, true>(a, grid, st) : launch_encode_t<uint32_t, false>(a, grid, st);
-  return lossy ? launch_encode_t<uint64_t, true>(a, grid, st) : launch_encode_t<uint64_t, false>(a, grid, st);
+  auto k = k_decode<T, LOSSY, S::NT, S::MINB>;
+  static unsigned long long attr = 0;
+  cudaError_t e = ensure_smem_attr(k, DEC_SMEM, &attr);
+  if (e != cudaSuccess) return e;
+  k<<<grid, S::NT, DEC_SMEM, st>>>(a);
+  return cudaGetLastError();
 }
+
+template <typename T, bool LOSSY, class S>
+static int dec_occupancy()
+{
+  auto k = k_decode<T, LOSSY, S::NT, S::MINB>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, S::NT, DEC_SMEM);
+  return n;
+}
+
+template <int KIND>
+static cudaError_t launch_enc_kind(int shape, const EncArgs& a, int grid, cudaStream_t st)
+{
+  switch (shape) {
+    case 1: return launch_enc_k<KIND, EncShape1>(a, grid, st);
+    case 2: return launch_enc_k<KIND, EncShape2>(a, grid, st);
+    default: return launch_enc_k<KIND, EncShape0>(a, grid, st);
+  }
+}
+
+template <int KIND>
+static int enc_occupancy_kind(int shape)
+{
+  switch (shape) {
+    case 1: return enc_occupancy<KIND, EncShape1>();
+    case 2: return enc_occupancy<KIND, EncShape2>();
+    default: return enc_occupancy<KIND, EncShape0>();
+  }
+}
+
+template <typename T, bool LOSSY>
+static cudaError_t launch_dec_kind(int shape, const DecArgs& a, int grid, cudaStream_t st)
+{
+  switch (shape) {
+    case 1: return launch_dec_k<T, LOSSY, DecShape1>(a, grid, st);
+    case 2: return launch_dec_k<T, LOSSY, DecShape2>(a, grid, st);
+    default: return launch_dec_k<T, LOSSY, DecShape0>(a, grid, st);
+  }
+}
+
+template <typename T, bool LOSSY>
+static int dec_occupancy_kind(int shape)
+{
+  switch (shape) {
+    case 1: return dec_occupancy<T, LOSSY, DecShape1>();
+    case 2: return dec_occupancy<T, LOSSY, DecShape2>();
+    default: return dec_occupancy<T, LOSSY, DecShape0>();
+  }
+}
+
+cudaError_t launch_encode(int width, bool lossy, int shape, const EncArgs& a, int grid, cudaStream_t st)
+{
+  if (width == 4) return lossy ? launch_enc_kind<2>(shape, a, grid, st) : launch_enc_kind<0>(shape, a, grid, st);
+  return lossy ? launch_enc_kind<3>(shape, a, grid, st) : launch_enc_kind<1>(shape, a, grid, st);
+}
+
+cudaError_t launch_decode(int width, bool lossy, int shape, const DecArgs& a, int grid, cudaStream_t st)
+{
+  if (width == 4)
+    return lossy ? launch_dec_kind<uint32_t, true>(shape, a, grid, st) : launch_dec_kind<uint32_t, false>(shape, a, grid, st);
+  return lossy ? launch_dec_kind<uint64_t, true>(shape, a, grid, st) : launch_dec_kind<uint64_t, false>(shape, a, grid, st);
+}
+
+int blocks_per_sm(int width, bool lossy, bool enc, int shape)
+{
+  if (enc) {
+    if (width == 4) return lossy ? enc_occupancy_kind<2>(shape) : enc_occupancy_kind<0>(shape);
+    return lossy ? enc_occupancy_kind<3>(shape) : enc_occupancy_kind<1>(shape);
+  }
+  if (width == 4) return lossy ? dec_occupancy_kind<uint32_t, true>(shape) : dec_occupancy_kind<uint32_t, false>(shape);
+  return lossy ? dec_occupancy_kind<uint64_t, true>(shape) : dec_occupancy_kind<uint64_t, false>(shape);
+}
+
+ShapeInfo shape_info(bool enc, int shape)
+{
+  ShapeInfo r{};
+  if (enc) {
+    switch (shape) {
+      case 1: r = {EncShape1::NT, EncShape1::CW, EncShape1::ST, EncShape1::MINB}; break;
+      case 2: r = {EncShape2::NT, EncShape2::CW, EncShape2::ST, EncShape2::MINB}; break;
+      default: r = {EncShape0::NT, EncShape0::CW, EncShape0::ST, EncShape0::MINB}; break;
+    }
+  } else {
+    switch (shape) {
+      case 1: r = {DecShape1::NT, DecShape1::NT / 32, DEC_STAGES, DecShape1::MINB}; break;
+      case 2: r = {DecShape2::NT, DecShape2::NT / 32, DEC_STAGES, DecShape2::MINB}; break;
+      default: r = {DecShape0::NT, DecShape0::NT / 32, DEC_STAGES, DecShape0::MINB}; break;
+    }
+  }
+  return r;
+}
+
+int shape_count(bool enc) { return enc ? ENC_SHAPES : DEC_SHAPES; }
 
 cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st)
 {
-  auto k = k_encode<-1, true, ENC_MINB>;
+  using S = EncShape0;
+  auto k = k_encode<-1, true, S>;
   static unsigned long long attr = 0;
-  cudaError_t e = ensure_smem_attr(k, ENC_BATCH_SMEM, &attr);
+  cudaError_t e = ensure_smem_attr(k, enc_batch_smem<S>(), &attr);
   if (e != cudaSuccess) return e;
-  k<<<grid, ENC_NT, ENC_BATCH_SMEM, st>>>(a);
+  k<<<grid, S::NT, enc_batch_smem<S>(), st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1315,39 +1463,11 @@ int decode_batch_blocks_per_sm()
 
 int encode_batch_blocks_per_sm()
 {
-  cudaFuncSetAttribute(k_encode<-1, true, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_BATCH_SMEM);
+  using S = EncShape0;
+  cudaFuncSetAttribute(k_encode<-1, true, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, enc_batch_smem<S>());
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<-1, true, ENC_MINB>, ENC_NT, ENC_BATCH_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode<-1, true, S>, S::NT, enc_batch_smem<S>());
   return n;
-}
-
-cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st)
-{
-  if (width == 4) return lossy ? launch_decode_t<uint32_t, true>(a, grid, st) : launch_decode_t<uint32_t, false>(a, grid, st);
-  return lossy ? launch_decode_t<uint64_t, true>(a, grid, st) : launch_decode_t<uint64_t, false>(a, grid, st);
-}
-
-int blocks_per_sm(int width, bool lossy, bool enc)
-{
-  // the smem attribute must be set before the occupancy query counts dynamic smem
-  if (width == 4) {
-    if (lossy) {
-      cudaFuncSetAttribute(k_encode<2, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
-      cudaFuncSetAttribute(k_decode<uint32_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
-      return occupancy_t<uint32_t, true>(enc);
-    }
-    cudaFuncSetAttribute(k_encode<0, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
-    cudaFuncSetAttribute(k_decode<uint32_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
-    return occupancy_t<uint32_t, false>(enc);
-  }
-  if (lossy) {
-    cudaFuncSetAttribute(k_encode<3, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
-    cudaFuncSetAttribute(k_decode<uint64_t, true, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
-    return occupancy_t<uint64_t, true>(enc);
-  }
-  cudaFuncSetAttribute(k_encode<1, false, ENC_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENC_SMEM);
-  cudaFuncSetAttribute(k_decode<uint64_t, false, 256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, DEC_SMEM);
-  return occupancy_t<uint64_t, false>(enc);
 }
 
 }  // namespace sleek

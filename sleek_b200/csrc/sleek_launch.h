@@ -24,7 +24,8 @@ struct EncArgs {
   long long insize;      // input bytes
   uint8_t* out;          // device stream, >= upper bound size, 8-byte aligned
   long long* outsize;    // device: stream bytes, or -status on a device-detected error
-  uint64_t* ws;          // zeroed workspace: header words + one flag per chunk
+  uint64_t* ws;          // workspace: header words + flag regions (self-resetting, see WsPhase)
+  long long flag_cap;    // flags per region (at least one per chunk)
   QParams q;
 };
 
@@ -34,7 +35,8 @@ struct DecArgs {
   uint8_t* out;          // device output values (element aligned)
   long long out_cap;     // output capacity in bytes, or -1 when unknown
   long long* outsize;    // device: decoded bytes, or -status
-  uint64_t* ws;          // zeroed workspace: header words + one flag per CTA
+  uint64_t* ws;          // workspace: header words + flag regions (self-resetting, see WsPhase)
+  long long flag_cap;    // flags per region (at least one per CTA)
   QParams q;
 };
 
@@ -70,13 +72,23 @@ struct BatchDecArgs {
   long long* actual_insize;     // workspace: bytes each stream decodes to
 };
 
-cudaError_t launch_encode(int width, bool lossy, const EncArgs& a, int grid, cudaStream_t st);
+// Launch shapes of the single-buffer kernels (sleek_kernels.cu: EncShape*,
+// DecShape*); shape 0 is the default.  Every shape produces the same bytes.
+struct ShapeInfo {
+  int threads;        // per CTA
+  int warps;          // compute warps (encode) / warps (decode)
+  int stages;         // shared-memory chunk stages
+  int ctas_per_sm;    // CTAs per SM the registers are budgeted for
+};
+int shape_count(bool enc);
+ShapeInfo shape_info(bool enc, int shape);
+cudaError_t launch_encode(int width, bool lossy, int shape, const EncArgs& a, int grid, cudaStream_t st);
+cudaError_t launch_decode(int width, bool lossy, int shape, const DecArgs& a, int grid, cudaStream_t st);
+int blocks_per_sm(int width, bool lossy, bool enc, int shape);
 cudaError_t launch_decode_batch(const BatchDecArgs& a, int grid, cudaStream_t st);
 int decode_batch_blocks_per_sm();
 cudaError_t launch_encode_batch(const BatchEncArgs& a, int grid, cudaStream_t st);
 int encode_batch_blocks_per_sm();
-cudaError_t launch_decode(int width, bool lossy, const DecArgs& a, int grid, cudaStream_t st);
-int blocks_per_sm(int width, bool lossy, bool enc);
 // the single-buffer entry points for other host sources of the library (they use
 // the library-owned workspace of `stream`); host_qparams derives the quantizer
 // parameters of an error bound (SLEEK_ERR_ERROR_BOUND when it is too large)

@@ -6,8 +6,11 @@
 // must not risk the implicit device synchronisation an allocation can cause.  For
 // them this entry point compresses with a scratch area that is part of the library
 // image itself: a file-scope __device__ array, allocated once per device when the
-// library's device code is loaded and held until the process exits.  The caller
-// still passes the input, the output stream buffer and the size output.
+// library's device code is loaded on that device (with lazy module loading, the
+// CUDA default, that happens at the first call's address lookup below, which is
+// why the first call belongs at initialisation time) and held until the process
+// exits.  The caller still passes the input, the output stream buffer and the size
+// output.
 //
 // The scratch holds the same things the regular entry point's workspace holds (a
 // header of 32 words and one look-back flag per 16 KB chunk), so its fixed size

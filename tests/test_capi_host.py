@@ -130,3 +130,19 @@ def test_batch_items_beyond_the_largest_input_are_rejected_on_the_host(elem):
         assert not plan.value
     it.num_elements = -1
     assert L.sleek_batch_plan_create(C.byref(it), 1, 0, C.byref(plan)) == _capi.SLEEK_ERR_INVALID_ARG
+
+
+def test_launch_shapes_are_described_and_validated_on_the_host():
+    L = _capi.lib()
+    t, w, s, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    for dec in (0, 1):
+        n = 0
+        while L.sleek_launch_shape_info(dec, n, C.byref(t), C.byref(w), C.byref(s), C.byref(c)) == 0:
+            assert t.value % 32 == 0 and 1 <= w.value <= t.value // 32 and s.value >= 2 and c.value >= 1
+            n += 1
+        assert n >= 2  # shape 0 (the default) and at least one alternative
+        assert L.sleek_launch_shape_info(dec, -1, None, None, None, None) == _capi.SLEEK_ERR_INVALID_ARG
+        assert L.sleek_set_launch_shape(dec, 4, 0, 20, n, 0) == _capi.SLEEK_ERR_INVALID_ARG
+        assert L.sleek_set_launch_shape(dec, 2, 0, 20, 0, 0) == _capi.SLEEK_ERR_INVALID_ARG
+        assert L.sleek_set_launch_shape(dec, 4, 0, 64, 0, 0) == _capi.SLEEK_ERR_INVALID_ARG
+        assert L.sleek_set_launch_shape(dec, 4, 0, 20, 0, -1) == _capi.SLEEK_ERR_INVALID_ARG

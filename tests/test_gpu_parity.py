@@ -205,6 +205,42 @@ def test_caller_workspace(cuda):
         api.sleek_compress_gpu(0, x, x.numel(), enc, size, workspace=small)
 
 
+def test_library_workspace_resets_itself_between_calls(cuda):
+    # The library-owned workspace of a stream is cleared once, when it is allocated;
+    # every launch then leaves the other half clean for the next one.  A run of calls
+    # whose chunk counts shrink and grow (growth past the first allocation included),
+    # with decompressions, range reductions and a failed call in between, must give
+    # the oracle's streams throughout.
+    from sleek_b200 import _capi
+    side = torch.cuda.Stream()
+    sh = side.cuda_stream
+    status = C.c_int(-1)
+    seq = [(700 * 4096 + 5, np.float32, None), (3 * 2048, np.float64, 1e-3), (1, np.float32, 1e-2),
+           (0, np.float64, None), (5000 * 4096 + 17, np.float32, None), (2 * 2048 + 1, np.float64, None),
+           (700 * 2048, np.float64, 1e-6), (9, np.float32, None)]
+    with torch.cuda.stream(side):
+        for k, (n, dt, eb) in enumerate(seq):
+            x = _mixed(max(n, 1), dt, 500 + k)[:n]
+            t = torch.from_numpy(x).cuda()
+            s = api.compress(t, eb)
+            want = O.encode(x, eb)
+            assert s.cpu().numpy().tobytes() == want, (k, n)
+            y = api.decompress(s, dt, eb)
+            assert y.cpu().numpy().tobytes() == O.decode(want, dt, eb).tobytes(), (k, n)
+            if n:
+                api.value_range(t)
+            if k == 3:  # a failed decode on the same workspace, then good calls again
+                b = bytearray(want if n else O.encode(_mixed(5000, dt, 9), eb))
+                b[8] = 0xFF
+                b[9] = 0x7F
+                with pytest.raises(SleekError):
+                    api.decompress(torch.frombuffer(b, dtype=torch.uint8).cuda(), dt, eb)
+                _capi.check(_capi.lib().sleek_workspace_status(None, sh, C.byref(status)))
+                assert status.value == _capi.SLEEK_ERR_CORRUPT_STREAM
+        _capi.check(_capi.lib().sleek_workspace_status(None, sh, C.byref(status)))
+        assert status.value == _capi.SLEEK_OK
+
+
 # ---- malformed streams: an error status, never a trap ----------------------------------
 
 def test_corrupt_streams_report_status(cuda):
