@@ -575,7 +575,7 @@ def _geomean(v):
     return float(np.exp(np.mean(np.log(v)))) if v else None
 
 
-def bench_configs(dev, peak, extra_rows=None, reps=10):
+def bench_configs(dev, peak, extra_rows=None, reps=10, tune=True):
     """Every single-buffer configuration of the measurement table on the same device
     path, each beside a D2D copy of the same bytes (the reference's own comparison,
     memcpy.cu:121-129, made per input by compress_decompress_inputs_single.py:228-240):
@@ -620,6 +620,12 @@ def bench_configs(dev, peak, extra_rows=None, reps=10):
                                                         size.data_ptr(), None, 0, sh)
                 fd = lambda: L.sleek_decompress_lossy_f32(e, enc.data_ptr(), enc.numel(), dec.data_ptr(), N,
                                                           size[1:].data_ptr(), None, 0, sh)
+            shapes = None
+            if tune:
+                from sleek_b200 import autotune
+
+                shapes = {d: _tuned_row(autotune.tune_single(x, eb, decompress=(d == "decompress"), use_cache=False))
+                          for d in ("compress", "decompress")}
             with torch.cuda.stream(side):
                 for _ in range(3):  # warm-up outside capture (grid sizes, attributes, workspace)
                     _capi.check(fc())
@@ -635,6 +641,8 @@ def bench_configs(dev, peak, extra_rows=None, reps=10):
             cg = _graph_gbs(lambda: _capi.check(fc()), N, reps, side)
             dg = _graph_gbs(lambda: _capi.check(fd()), N, reps, side)
             row[str(eb)] = _mode_row(N, S, cg, dg, memcpy, peak)
+            if shapes:
+                row[str(eb)]["launch_shapes"] = shapes
         out[name] = row
         del x, enc, dec
         torch.cuda.empty_cache()
@@ -650,6 +658,13 @@ def bench_configs(dev, peak, extra_rows=None, reps=10):
                                          for k in ("compress", "decompress")}
     out["timing"] = f"{reps} calls per CUDA graph replay, CUDA events; copy: {reps} D2D copies of the same bytes"
     return out
+
+
+def _tuned_row(r):
+    """The autotuner's choice as recorded in the bench line."""
+    sh = r["shape"]
+    return {"shape": sh["shape"], "threads": sh["threads"], "warps": sh["warps"], "stages": sh["stages"],
+            "ctas_per_sm": r["best"][1] or "all that fit", "size_bucket_log2": r["bucket_log2"]}
 
 
 def _mode_row(N, S, cg, dg, memcpy, peak):
@@ -726,6 +741,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1000-array) comparison")
     ap.add_argument("--no-transfer", action="store_true", help="skip the compressed host<->device copy leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the f32 configurations leg")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes, no autotuning")
     ap.add_argument("--serve-requests", type=int, default=100000,
                     help="requests of the served workload leg (0 = skip; 100000 = the full workload)")
     args = ap.parse_args()
@@ -773,6 +789,17 @@ def main():
             rc = L.sleek_decompress_lossy_f64(ebi[i], enc[i].data_ptr(), cap, dec.data_ptr(), N,
                                               dsz[i:].data_ptr(), None, 0, sh)
         _capi.check(rc, "decompress")
+
+    # launch shapes: the autotuner times the kernel shapes on this field, per mode and
+    # direction, and the timed calls below use its choice
+    tuned = {}
+    if not args.no_tune:
+        from sleek_b200 import autotune
+
+        for i, eb in enumerate(MODES):
+            tuned[str(eb)] = {d: _tuned_row(autotune.tune_single(x, eb, decompress=(d == "decompress"),
+                                                                 use_cache=False))
+                              for d in ("compress", "decompress")}
 
     # correctness gate before timing: every mode round-trips and sizes are sane
     for i in range(len(MODES)):
@@ -944,6 +971,7 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * len(MODES) * args.steps,
         "clocks": clocks,
+        "launch_shapes": tuned or "defaults (--no-tune)",
     }
     if not args.no_batched:
         # free the single-buffer leg's buffers first
@@ -960,7 +988,11 @@ def main():
         c1_row = {"bytes": N, "memcpy_d2d_gbs": round(memcpy_gbs, 1)}
         for i, m in enumerate(MODES):
             c1_row[str(m)] = _mode_row(N, S[i], N / (tc[i] * 1e-3) / 1e9, N / (td[i] * 1e-3) / 1e9, memcpy_gbs, peak)
-        line["configs"] = bench_configs(dev, peak, {"c1 f64 256x384x384 (main leg, per-call CUDA events)": c1_row})
+        for i, m in enumerate(MODES):
+            if tuned:
+                c1_row[str(m)]["launch_shapes"] = tuned[str(m)]
+        line["configs"] = bench_configs(dev, peak, {"c1 f64 256x384x384 (main leg, per-call CUDA events)": c1_row},
+                                        tune=not args.no_tune)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference's own implementations on this box: its CPU codec (the baseline)
         # and, beside it, its GPU kernels built for sm_100a; the oracle checks the
