@@ -24,6 +24,7 @@ import json
 import os
 from typing import Callable, Dict, List, Optional, Sequence
 
+import numpy as np
 import torch
 
 from . import _capi
@@ -118,7 +119,7 @@ def tune_single(x: torch.Tensor, eb: Optional[float], decompress: bool = False, 
     nbytes = x.numel() * w
     bucket = size_log2(nbytes)
     enc = api.compress(x, eb)
-    dt = torch.float32 if w == 4 else torch.float64
+    dt = np.float32 if w == 4 else np.float64
     out = torch.empty_like(x)
 
     def apply(c):

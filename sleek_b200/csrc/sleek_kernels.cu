@@ -859,6 +859,8 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   const WsPhase ph = WsPhase::of(a.ws, a.flag_cap);  // self-resetting workspace
   uint64_t* const hdr = ph.hdr;
   uint64_t* const flags = ph.flags;
+  // this CTA's share of the flags the previous launch left in the other region
+  if (warp == NW - 1) ph.clear_other_share(lane);
 
   // header checks (every CTA reads the 8-byte header)
   const long long insize = *reinterpret_cast<const long long*>(a.in);
