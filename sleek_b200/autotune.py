@@ -110,27 +110,39 @@ def size_log2(nbytes: int) -> int:
 
 def tune_single(x: torch.Tensor, eb: Optional[float], decompress: bool = False, use_cache: bool = True) -> dict:
     """Tunes and applies the launch shape and CTAs per SM of the single-buffer kernel
-    of x's kind for inputs in x's size bucket."""
+    of x's kind for inputs in x's size bucket.  Candidates are timed on the device:
+    C-ABI calls into preallocated buffers, back to back on the current stream (no
+    host wait between calls, so small inputs are not timed by the host's latency)."""
     from . import api
 
     L = _capi.lib()
     w = x.element_size()
     lossy = int(eb is not None)
+    x = x.contiguous().view(-1)
     nbytes = x.numel() * w
     bucket = size_log2(nbytes)
+    t = "f32" if w == 4 else "f64"
     enc = api.compress(x, eb)
-    dt = np.float32 if w == 4 else np.float64
     out = torch.empty_like(x)
+    buf = torch.empty(api.sleek_upper_bound_size(nbytes), dtype=torch.uint8, device=x.device)
+    size = torch.zeros(1, dtype=torch.int64, device=x.device)
+    pre = (api.sleek_error_bound(eb, np.float32 if w == 4 else np.float64).c_struct(),) if lossy else ()
+    mid = "_lossy" if lossy else ""
+    fc = getattr(L, f"sleek_compress{mid}_{t}")
+    fd = getattr(L, f"sleek_decompress{mid}_{t}")
 
     def apply(c):
         _capi.check(L.sleek_set_launch_shape(int(decompress), w, lossy, bucket, c[0], c[1]), "sleek_set_launch_shape")
 
     def run(c):
         apply(c)
-        if decompress:
-            api.decompress(enc, dt, eb, out=out)
-        else:
-            api.compress(x, eb)
+        sh = torch.cuda.current_stream().cuda_stream
+        for _ in range(4):
+            if decompress:
+                rc = fd(*pre, enc.data_ptr(), enc.numel(), out.data_ptr(), nbytes, size.data_ptr(), None, 0, sh)
+            else:
+                rc = fc(*pre, x.data_ptr(), x.numel(), buf.data_ptr(), size.data_ptr(), None, 0, sh)
+            _capi.check(rc)
 
     key = f"single|{'dec' if decompress else 'enc'}|{w}|{lossy}|2^{bucket}"
     r = tune(key, run, single_candidates(decompress), use_cache=use_cache)

@@ -22,15 +22,18 @@ constexpr unsigned ST_CORRUPT = 5;
 constexpr unsigned ST_TIMEOUT = 6;
 constexpr unsigned ST_CAPACITY = 9;
 
-// Workspace: 32 header words (u64 each), then the look-back flags.  The header
-// holds two blocks of per-launch counters (words 0-7 and 8-15), the launch epoch
-// (word 16) and words the range reduction uses (24-26).  Single-buffer launches
-// alternate between the blocks and between two flag regions by epoch parity (see
-// WsPhase below); batched launches use block 0 and the first region of a
-// workspace cleared before each run.
+// Workspace: 32 header words (u64 each), then the look-back flags.  Words 0 and
+// 1 are the launch's ticket and done counters; two blocks of per-launch results
+// (status, total, error position, flags used) follow at words 0-7 and 8-15 (the
+// first block shares its first two words with the counters), then the launch
+// epoch (word 16) and words the range reduction uses (24-26).  Single-buffer
+// launches alternate between the blocks and between two flag regions by epoch
+// parity (see WsPhase below); batched launches use block 0 and the first region
+// of a workspace cleared before each run.
 enum WsWord {
-  WS_TICKET = 0, WS_DONE = 1, WS_STATUS = 2, WS_TOTAL = 3, WS_ERRPOS = 4, WS_USED = 5,  // within a block
-  WS_BLOCK = 8,       // words per counter block
+  WS_TICKET = 0, WS_DONE = 1,                                   // counters (words 0, 1)
+  WS_STATUS = 2, WS_TOTAL = 3, WS_ERRPOS = 4, WS_USED = 5,      // within a block
+  WS_BLOCK = 8,       // words per block
   WS_EPOCH = 16,      // launches completed on this workspace
   WS_MINMAX = 24,     // three words for the range reduction (cleared by its own call)
   WS_HDR_WORDS = 32
@@ -173,13 +176,15 @@ __device__ __forceinline__ void set_status(uint64_t* hdr, unsigned code, long lo
 
 // ----------------------------------------------------------------------------
 // Self-resetting workspace of the single-buffer kernels.  A launch works in
-// counter block and flag region p = epoch & 1 (both clean when it starts), and
+// result block and flag region p = epoch & 1 (both clean when it starts), and
 // leaves the other parity clean for the next launch: every CTA clears its share
 // of the flags the previous launch used there, and the last CTA resets that
-// counter block, records how many flags this launch used, then advances the
-// epoch.  A workspace that starts zeroed therefore needs no clearing between
-// launches on one stream; a workspace cleared before every launch (epoch 0)
-// behaves the same.  flag_cap is the size of one flag region.
+// block and the ticket and done counters, records how many flags this launch
+// used, then advances the epoch.  The counters do not depend on the epoch, so a
+// CTA takes its first ticket without waiting for the epoch's load.  A workspace
+// that starts zeroed therefore needs no clearing between launches on one stream;
+// a workspace cleared before every launch (epoch 0) behaves the same.  flag_cap
+// is the size of one flag region.
 // ----------------------------------------------------------------------------
 struct WsPhase {
   uint64_t* hdr;        // this launch's counter block
@@ -225,12 +230,15 @@ struct WsPhase {
     for (long long i = b + lane; i < e; i += 32) flags_other[i] = 0ull;
   }
 
-  // the last CTA, one thread, after every CTA has counted itself done
+  // the last CTA, one thread, after every CTA has counted itself done (so no
+  // ticket or done atomic of this launch is still to come)
   __device__ void finish(uint64_t* ws, long long used) const
   {
     hdr[WS_USED] = static_cast<uint64_t>(used);
 #pragma unroll
-    for (int i = 0; i < WS_BLOCK; ++i) hdr_other[i] = 0ull;
+    for (int i = WS_STATUS; i < WS_BLOCK; ++i) hdr_other[i] = 0ull;
+    ws[WS_TICKET] = 0ull;
+    ws[WS_DONE] = 0ull;
     __threadfence();
     ws[WS_EPOCH] = epoch + 1u;
   }
@@ -597,12 +605,13 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
 }
 
 // ----------------------------------------------------------------------------
-// Shifted store by one warp: writes `len` bytes from 16-byte aligned shared
-// memory `src` to the arbitrary global byte address `dst`.  The whole aligned
-// 16-byte granules go out in 32-byte aligned pairs, one 256-bit store each,
-// funnel-shifted from three aligned shared loads, consecutive lanes on
-// consecutive pairs (a warp instruction fills whole lines); the at most two
-// granules shared with neighbouring chunks are written byte by byte.
+// Shifted store by NT threads (t = 0 .. NT-1): writes `len` bytes from 16-byte
+// aligned shared memory `src` to the arbitrary global byte address `dst`.  The
+// whole aligned 16-byte granules go out in 32-byte aligned pairs, one 256-bit
+// store each, funnel-shifted from three aligned shared loads, consecutive threads
+// on consecutive pairs (a warp instruction fills whole lines); at most two
+// unpaired granules take a 16-byte store, and the at most two granules shared
+// with the neighbouring chunks are written byte by byte by the first warp.
 // ----------------------------------------------------------------------------
 template <int WQ>
 __device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, int bb8)
@@ -633,16 +642,14 @@ __device__ __forceinline__ uint4 out_granule(const uint4* s4, int j, int bb8)
   else return shifted_granule<WQ>(s4[j - 1], s4[j], bb8);
 }
 
-// Granules jf .. jl-1 of the output: 32-byte aligned pairs, one per lane and
-// iteration (consecutive lanes on consecutive pairs), each from three aligned
-// shared loads; the at most two unpaired granules by lanes 0 and 1.
-template <int WQ>
-__device__ __forceinline__ void shifted_pairs_warp(uint4* out, const uint4* s4, int jf, int jl, int bb8, int par,
-                                                   int lane)
+// Granules jf .. jl-1 of the output: 32-byte aligned pairs, one per thread and
+// iteration; the at most two unpaired granules by threads 0 and 1.
+template <int WQ, int NT>
+__device__ __forceinline__ void shifted_pairs(uint4* out, const uint4* s4, int jf, int jl, int bb8, int par, int t)
 {
   const int jp = jf + ((jf + par) & 1);  // first granule that starts a 32-byte aligned pair
   const int np = jl - jp >= 0 ? (jl - jp) >> 1 : 0;
-  for (int k = lane; k < np; k += 32) {
+  for (int k = t; k < np; k += NT) {
     const int j = jp + 2 * k;
     if constexpr (WQ < 0) {
       st_global_v8(out + j, s4[j], s4[j + 1]);
@@ -652,12 +659,13 @@ __device__ __forceinline__ void shifted_pairs_warp(uint4* out, const uint4* s4, 
     }
   }
   int j = -1;
-  if (lane == 0 && jp > jf && jf < jl) j = jf;
-  if (lane == 1 && jp + 2 * np < jl) j = jp + 2 * np;
+  if (t == 0 && jp > jf && jf < jl) j = jf;
+  if (t == 1 && jp + 2 * np < jl) j = jp + 2 * np;
   if (j >= 0) out[j] = out_granule<WQ>(s4, j, bb8);
 }
 
-__device__ __forceinline__ void store_shifted_warp(uint8_t* dst, const uint8_t* src, int len, int lane)
+template <int NT>
+__device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len, int t)
 {
   const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
   const int sft = static_cast<int>(d & 15u);
@@ -669,29 +677,31 @@ __device__ __forceinline__ void store_shifted_warp(uint8_t* dst, const uint8_t* 
   const int jf = sft ? 1 : 0;              // first granule entirely inside the chunk
   const int jl = (sft + len) >> 4;         // one past the last such granule
   if (sft == 0) {
-    shifted_pairs_warp<-1>(out, s4, jf, jl, 0, par, lane);
+    shifted_pairs<-1, NT>(out, s4, jf, jl, 0, par, t);
   } else {
     const int bo = 16 - sft;
     const int bb8 = (bo & 3) * 8;
     switch (bo >> 2) {
-      case 0: shifted_pairs_warp<0>(out, s4, jf, jl, bb8, par, lane); break;
-      case 1: shifted_pairs_warp<1>(out, s4, jf, jl, bb8, par, lane); break;
-      case 2: shifted_pairs_warp<2>(out, s4, jf, jl, bb8, par, lane); break;
-      default: shifted_pairs_warp<3>(out, s4, jf, jl, bb8, par, lane); break;
+      case 0: shifted_pairs<0, NT>(out, s4, jf, jl, bb8, par, t); break;
+      case 1: shifted_pairs<1, NT>(out, s4, jf, jl, bb8, par, t); break;
+      case 2: shifted_pairs<2, NT>(out, s4, jf, jl, bb8, par, t); break;
+      default: shifted_pairs<3, NT>(out, s4, jf, jl, bb8, par, t); break;
     }
   }
-  // edge granules (shared with the neighbouring chunks): one byte per lane,
-  // lanes 0-15 the first granule, lanes 16-31 the last
-  int e = -1;
-  if (lane < 16) {
-    if (sft != 0) e = 0;
-  } else {
-    const int last = nunits - 1;
-    if (last >= jl && !(last == 0 && sft != 0)) e = last;
-  }
-  if (e >= 0) {
-    const int r = 16 * e - sft + (lane & 15);  // source byte of this lane
-    if (r >= 0 && r < len) a0[16 * e + (lane & 15)] = src[r];
+  // edge granules (shared with the neighbouring chunks): one byte per lane of the
+  // first warp, lanes 0-15 the first granule, lanes 16-31 the last
+  if (t < 32) {
+    int e = -1;
+    if (t < 16) {
+      if (sft != 0) e = 0;
+    } else {
+      const int last = nunits - 1;
+      if (last >= jl && !(last == 0 && sft != 0)) e = last;
+    }
+    if (e >= 0) {
+      const int r = 16 * e - sft + (t & 15);  // source byte of this lane
+      if (r >= 0 && r < len) a0[16 * e + (t & 15)] = src[r];
+    }
   }
 }
 

@@ -28,29 +28,31 @@
 namespace sleek {
 
 // Launch shape of the encode kernel: CW compute warps (each takes SC / CW
-// subchunks of a chunk), ST shared-memory stages of one chunk each, and a
-// producer that takes chunk k's ticket and issues its copy once the compute warps
-// have begun chunk k - AHEAD (and the stage's previous chunk is stored), so
-// tickets are taken at most AHEAD chunks ahead of the compute warps.  MINB is the
-// CTAs per SM the registers are budgeted for.  Every shape writes the same bytes.
-template <int CW_, int ST_, int AHEAD_, int MINB_>
+// subchunks of a chunk) and ST shared-memory stages of one chunk each.  The
+// compute warps store chunk k - LAG after computing chunk k (LAG = ST - 2: its
+// look-back gets LAG chunks of compute time), and the stage that store frees takes
+// chunk k + AHEAD (AHEAD = ST - LAG = 2: the producer runs one chunk ahead).
+// MINB is the CTAs per SM the registers are budgeted for.  Every shape writes the
+// same bytes.
+template <int CW_, int ST_, int MINB_>
 struct EncShape {
   static constexpr int CW = CW_;
   static constexpr int ST = ST_;
-  static constexpr int AHEAD = AHEAD_;
+  static constexpr int LAG = ST - 2;
+  static constexpr int AHEAD = ST - LAG;
   static constexpr int MINB = MINB_;
-  static constexpr int NT = (CW + 2) * 32;  // + a producer warp and a placer warp
+  static constexpr int NT = (CW + 2) * 32;  // + a producer warp and a scanner warp
   static constexpr int SPW = SC / CW;       // subchunks per compute warp
-  static_assert(SC % CW == 0 && AHEAD >= 1 && AHEAD < ST, "shape");
+  static_assert(SC % CW == 0 && LAG >= 1, "shape");
 };
 // the shapes the library is built with (index = the C ABI's shape number)
-using EncShape0 = EncShape<8, 4, 2, 3>;   // default: 10 warps, 66 KB, 3 CTAs per SM
-using EncShape1 = EncShape<16, 4, 2, 2>;  // 18 warps, 66 KB, 2 CTAs per SM
-using EncShape2 = EncShape<4, 4, 2, 3>;   // 6 warps, 66 KB, 3 CTAs per SM
+using EncShape0 = EncShape<8, 4, 3>;   // default: 10 warps, 66 KB, 3 CTAs per SM
+using EncShape1 = EncShape<16, 4, 2>;  // 18 warps, 66 KB, 2 CTAs per SM
+using EncShape2 = EncShape<4, 4, 3>;   // 6 warps, 66 KB, 3 CTAs per SM
 constexpr int ENC_SHAPES = 3;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
-// What the producer tells the compute and placer warps about the chunk in a stage.
+// What the producer tells the compute and scanner warps about the chunk in a stage.
 struct EncMeta {
   long long g;          // look-back flag index (chunk id across the launch), or NO_CHUNK
   long long c;          // chunk index within its buffer
@@ -59,7 +61,7 @@ struct EncMeta {
   long long insize;     // bytes of the buffer
   uint8_t* out;         // the buffer's stream
   long long* outsize;   // the buffer's size output
-  long long excl;       // payload offset of the chunk (placer), -1 after an error
+  long long excl;       // payload offset of the chunk (scanner), -1 after an error
   QParams q;            // the buffer's quantizer parameters
   int kind;             // bit 0: 64-bit values, bit 1: lossy
   int osize;
@@ -70,10 +72,9 @@ struct EncMeta {
 template <int ST>
 struct EncMisc {
   uint64_t full[ST];    // chunk bytes landed (TMA tx count)
-  uint64_t empty[ST];   // the stage's chunk is stored (placer): the stage may be refilled
-  uint64_t began[ST];   // the compute warps are past phase A of the stage's chunk
+  uint64_t empty[ST];   // go-ahead for the stage's next copy (its previous chunk is stored)
   uint64_t sized[ST];   // compressed size of the stage's chunk known
-  uint64_t packed[ST];  // every compute warp has packed its share of the stage's chunk
+  uint64_t placed[ST];  // payload offset of the stage's chunk known
   EncMeta meta[ST];
   int lnv[2][SC];  // subchunk bit widths, by chunk parity (a fast warp may write the next chunk's)
 };
@@ -404,7 +405,6 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc<
     me.comp = comp;
     st_relaxed_u64(&flags[me.g], (me.c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
     mbar_arrive(&m.sized[s]);
-    mbar_arrive(&m.began[s]);
   }
 
   // ---- pack this chunk from registers ----------------------------------------
@@ -487,6 +487,7 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
 {
   constexpr int ENC_STAGES = S::ST;
   constexpr int ENC_AHEAD = S::AHEAD;
+  constexpr int ENC_LAG = S::LAG;
   constexpr int ENC_CW = S::CW;
   constexpr int ENC_NT = S::NT;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -513,10 +514,9 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
   if (tid == 0) {
     for (int s = 0; s < ENC_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
-      mbar_init(&m.empty[s], 1);
-      mbar_init(&m.began[s], 1);
+      mbar_init(&m.empty[s], ENC_CW);  // one arrival per compute warp
       mbar_init(&m.sized[s], 1);
-      mbar_init(&m.packed[s], ENC_CW);  // one arrival per compute warp
+      mbar_init(&m.placed[s], 1);
     }
     mbar_fence_init();
   }
@@ -533,22 +533,21 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
     // look-back wait for it.
-    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&hdr[WS_TICKET]);
+    unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]);
     unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
     unsigned issued_par = 0;  // parity of that use
     bool more = true;
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      // The copy for chunk seq is issued once the compute warps are past phase A
-      // of chunk seq - ENC_AHEAD and the placer has stored the stage's previous
-      // chunk, seq - ENC_STAGES.
-      bool ok = true;
-      if (seq >= ENC_AHEAD)
-        ok = mbar_wait_bounded(&m.began[(seq - ENC_AHEAD) % ENC_STAGES], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
-      if (ok && seq >= ENC_STAGES) ok = mbar_wait_bounded(&m.empty[s], ((seq / ENC_STAGES) - 1) & 1);
-      if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
-        break;
+      // From seq ENC_AHEAD on, the copy for chunk seq is issued once every compute
+      // warp has finished chunk seq - ENC_AHEAD, in which the stage's previous
+      // chunk, seq - ENC_STAGES, was stored.
+      if (seq >= ENC_AHEAD) {
+        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+          if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+          break;
+        }
       }
       long long t = NO_CHUNK;
       if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
@@ -607,9 +606,7 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
         if (issued & (1u << s)) mbar_wait_bounded(&m.full[s], (issued_par >> s) & 1u);
     }
   } else if (warp == ENC_CW + 1) {
-    // ============ placer warp: decoupled look-back, then the chunk's store ============
-    // The compute warps never wait for a chunk's offset: they pack it and move on,
-    // and this warp places it once its look-back is done.
+    // ===================== scanner warp: decoupled look-back =====================
     if constexpr (!BATCH) ph.clear_other_share(lane);
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
@@ -636,7 +633,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
         if (err) excl = -1;
       }
       const int csize = me.csize;
-      uint8_t* const out = me.out;
       if (lane == 0) {
         if (c > 0) {
           if (err) set_status(hdr, err, g);
@@ -644,38 +640,53 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
           // every later chunk still writes inside the output bound
           st_relaxed_u64(&flags[g], FLAG_INC | static_cast<uint64_t>(excl >= 0 ? excl + csize : (c + 1) * CS));
         }
+        me.excl = excl;
         if (c == me.chunks - 1 && excl >= 0) {
           if constexpr (BATCH) {  // the buffer is complete: its header and size
-            *reinterpret_cast<long long*>(out) = me.insize;
+            *reinterpret_cast<long long*>(me.out) = me.insize;
             *me.outsize = 8 + 2 * me.chunks + excl + csize;
           } else {
             hdr[WS_TOTAL] = static_cast<uint64_t>(excl + csize);
           }
         }
+        mbar_arrive(&m.placed[s]);
       }
-      // the compute warps' packed bytes (or the raw chunk) are complete in the stage
-      ok = mbar_wait_bounded(&m.packed[s], par);
-      if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) set_status(hdr, ST_TIMEOUT, g);
-        break;
-      }
-      if (excl >= 0) {
-        store_shifted_warp(out + 8 + 2 * me.chunks + excl, stage0 + s * STAGE_BYTES, csize, lane);
-        if (lane == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
-      }
-      // the producer may refill the stage (generic reads ordered before its TMA write)
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&m.empty[s]);
     }
   } else {
     // ===================== compute warps =====================
-    // Warps pass each other freely between the barriers of compute_chunk: each
-    // waits for its stage itself and reports its share of a chunk packed with its
-    // own arrival; the placer stores the chunk once every warp has.
     const int cw = warp;
+    auto store = [&](int sq) {  // all compute threads; placed[] already observed
+      const int sp = sq % ENC_STAGES;
+      const EncMeta& me = m.meta[sp];
+      const long long excl = me.excl;
+      if (excl >= 0) {
+        uint8_t* const out = me.out;
+        const long long c = me.c;
+        const int csize = me.csize;
+        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize, tid);
+        if (tid == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
+      }
+    };
+
+    // Each thread waits for the offset itself; a wait that gives up skips this
+    // thread's share of the store and is reported at the next barrier.
+    auto placed_store = [&](int sq) -> bool {
+      if (!mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1)) {
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+        return false;
+      }
+      store(sq);
+      return true;
+    };
+
+    // Warps pass each other freely between the barriers of compute_chunk: each
+    // waits for its stage and its offsets itself and frees a stage with its own
+    // arrival, and the pack data one warp stores were written by the others
+    // before an earlier barrier.
+    int seq = 0;
+    bool failed = false;
     bool late = false;  // a wait of this thread gave up
-    for (int seq = 0;; ++seq) {
+    for (;; ++seq) {
       const int s = seq % ENC_STAGES;
       if (!mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1)) {
         if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
@@ -697,10 +708,25 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
           default: r = compute_chunk<3, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
         }
       }
-      if (r != 0) break;  // the end, or a wait that gave up (reported)
-      // this warp's share of the chunk is packed (its shared stores before the arrival)
+      if (r == 2) {
+        failed = true;
+        break;
+      }
+      if (r == 1) break;
+      // ---- store the chunk of seq - ENC_LAG once its offset is known -----------
+      // (waiting here rather than before the compute gives its look-back ENC_LAG
+      // chunks of compute time to finish)
+      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) late = true;
+      // this warp is done with the stage of seq - ENC_LAG, which the producer may
+      // now refill with chunk seq + ENC_AHEAD (generic accesses ordered before its TMA write)
+      fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&m.packed[s]);
+      if (lane == 0) mbar_arrive(&m.empty[(seq + ENC_AHEAD) % ENC_STAGES]);
+    }
+    if (!failed) {
+      // drain: chunks seq - ENC_LAG .. seq - 1
+      for (int q = seq >= ENC_LAG ? seq - ENC_LAG : 0; q < seq; ++q)
+        if (!placed_store(q)) break;
     }
   }
 
@@ -709,7 +735,7 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
   __shared__ int last_cta;
   if (tid == 0) {
     __threadfence();
-    const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_DONE]), 1ull);
+    const unsigned long long d = atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_DONE]), 1ull);
     last_cta = d == gridDim.x - 1;
     if (last_cta) __threadfence();
   }
@@ -878,7 +904,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       mbar_init(&m.empty[st], NW);  // one arrival per warp
     }
     mbar_fence_init();
-    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_TICKET]), 1ull));
+    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]), 1ull));
     if (!hdr_ok) set_status(hdr, ST_CORRUPT, -1);
     else if (!cap_ok) set_status(hdr, ST_CAPACITY, -1);
   }
@@ -1032,7 +1058,7 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   __syncthreads();
   if (tid == 0) {
     __threadfence();
-    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&hdr[WS_DONE]), 1ull);
+    const unsigned long long dn = atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_DONE]), 1ull);
     if (dn == gridDim.x - 1) {
       __threadfence();
       const unsigned long long st = ld_relaxed_u64(&hdr[WS_STATUS]);

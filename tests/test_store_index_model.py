@@ -1,19 +1,19 @@
-"""CPU model of the placer warp's store (store_shifted_warp in
+"""CPU model of the encoder's chunk store (store_shifted in
 sleek_b200/csrc/sleek_device.cuh): the chunk's bytes, staged at a 16-byte aligned
 shared-memory address, go to an arbitrary global byte address as 32-byte aligned
 pair stores (three staged granules each), at most two single 16-byte granules, and
 byte stores for the two granules shared with the neighbouring chunks.  The model
-repeats the kernel's index arithmetic lane by lane and checks, for every byte
-misalignment, both pair parities and chunk lengths from 1 byte to a full raw chunk:
-every destination byte is written exactly once, nothing outside the chunk's bytes
-is written, every pair store is 32-byte aligned, and every staged read stays inside
-the written bytes' granules and the stage."""
+repeats the kernel's index arithmetic thread by thread (the compute warps' 256
+threads, and one warp) and checks, for every byte misalignment, both pair parities
+and chunk lengths from 1 byte to a full raw chunk: every destination byte is written
+exactly once, nothing outside the chunk's bytes is written, every pair store is
+32-byte aligned, and every staged read stays inside the stage."""
 import pytest
 
 STAGE_BYTES = 16384 + 64
 
 
-def model(sft, par, ln):
+def model(sft, par, ln, nt):
     a0 = 16 * (2 + par)  # a 16-byte aligned base whose granule index has parity `par`
     dst = a0 + sft
     nunits = (sft + ln + 15) >> 4
@@ -26,8 +26,8 @@ def model(sft, par, ln):
 
     jp = jf + ((jf + par) & 1)
     np_ = (jl - jp) >> 1 if jl - jp >= 0 else 0
-    for lane in range(32):
-        for k in range(lane, np_, 32):
+    for lane in range(nt):
+        for k in range(lane, np_, nt):
             j = jp + 2 * k
             pairs.append(a0 + 16 * j)
             reads.update((j - 1, j, j + 1) if sft else (j, j + 1))
@@ -42,6 +42,8 @@ def model(sft, par, ln):
             reads.update((j - 1, j) if sft else (j,))
             for b in range(16):
                 wr(a0 + 16 * j + b)
+        if lane >= 32:
+            continue
         e = -1
         if lane < 16:
             if sft != 0:
@@ -60,11 +62,12 @@ def model(sft, par, ln):
 LENGTHS = list(range(1, 200)) + [255, 256, 257, 511, 512, 513, 1000, 4097, 8000, 16383 - 17, 16383, 16384]
 
 
+@pytest.mark.parametrize("nt", [32, 256])
 @pytest.mark.parametrize("sft", range(16))
-def test_store_writes_every_byte_once_and_nothing_else(sft):
+def test_store_writes_every_byte_once_and_nothing_else(sft, nt):
     for par in (0, 1):
         for ln in LENGTHS:
-            dst, written, reads, pairs = model(sft, par, ln)
+            dst, written, reads, pairs = model(sft, par, ln, nt)
             assert all(written.get(b, 0) == 1 for b in range(dst, dst + ln)), (sft, par, ln)
             assert all(dst <= b < dst + ln for b in written), (sft, par, ln)
             assert all(p % 32 == 0 for p in pairs), (sft, par, ln)
