@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
         uint8_t* const out = me.out;
         const long long c = me.c;
         const int csize = me.csize;
-        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize, tid);
+        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize);
         if (tid == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
       }
     };
@@ -785,8 +785,14 @@ struct DecMisc {
   long long excl;
   long long vb;
   long long red[NT_MAX_WARPS];
+  long long pre[NT_MAX_WARPS];
   int bad[NT_MAX_WARPS];
 };
+
+// Streams of at most this many chunks place each CTA's range by summing the size
+// table before it directly (at most 8 KB read per CTA, no wait on other CTAs)
+// instead of the decoupled look-back, whose chain of polls dominates small decodes.
+constexpr long long DEC_DIRECT_MAX = 4096;
 
 constexpr int DEC_SMEM = DEC_STAGES * STAGE_BYTES + ((sizeof(DecMisc) + 127) / 128) * 128;
 
@@ -918,7 +924,8 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
 
   // ---- range aggregate + size-table validation ---------------------------------
   {
-    long long sum = 0;
+    const bool direct = go && chunks <= DEC_DIRECT_MAX;
+    long long sum = 0, pre = 0;
     int bad = 0;
     for (long long c = c0 + tid; c < c1; c += NT) {
       const int cs = size_in[c];
@@ -926,10 +933,23 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
       sum += cs;
     }
+    if (direct) {
+      // sizes [0, c0), four per 8-byte load (the table starts 8-byte aligned)
+      const unsigned long long* const s8 = reinterpret_cast<const unsigned long long*>(size_in);
+      const long long q = c0 >> 2;
+      for (long long k = tid; k < q; k += NT) {
+        const unsigned long long v = s8[k];
+        const unsigned long long p2 = (v & 0x0000ffff0000ffffull) + ((v >> 16) & 0x0000ffff0000ffffull);
+        pre += static_cast<long long>((p2 & 0xffffffffull) + (p2 >> 32));
+      }
+      for (long long c = (q << 2) + tid; c < c0; c += NT) pre += size_in[c];
+      pre = warp_sum(pre);
+    }
     sum = warp_sum(sum);
     bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
       m.red[warp] = sum;
+      m.pre[warp] = pre;
       m.bad[warp] = bad;
     }
     __syncthreads();
@@ -939,9 +959,14 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       s2 = warp_sum(s2);
       b2 = __any_sync(0xffffffffu, b2);
       if (b2 && lane == 0) set_status(hdr, ST_CORRUPT, c0);
-      if (lane == 0) st_relaxed_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
       long long excl = 0;
-      if (vb > 0) {
+      if (direct) {
+        excl = warp_sum(lane < NW ? m.pre[lane] : 0);
+      } else {
+        if (lane == 0)
+          st_relaxed_u64(&flags[vb], (vb == 0 ? FLAG_INC : FLAG_AGG) | (static_cast<uint64_t>(s2) & FLAG_VAL));
+      }
+      if (!direct && vb > 0) {
         excl = lookback(flags, vb, 0, hdr);
         if (excl < 0) {
           if (lane == 0) set_status(hdr, ST_TIMEOUT, c0);
