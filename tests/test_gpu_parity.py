@@ -241,6 +241,50 @@ def test_library_workspace_resets_itself_between_calls(cuda):
         assert status.value == _capi.SLEEK_OK
 
 
+def test_graph_replays_with_the_library_workspace(cuda):
+    # Captured calls keep their workspace pointer; the workspace's epoch lives on the
+    # device, so replaying the graph many times (encodes and decodes of different
+    # sizes alternating on one stream) keeps every output equal to the oracle's.
+    from sleek_b200 import _capi
+    L = _capi.lib()
+    side = torch.cuda.Stream()
+    sh = side.cuda_stream
+    xs = [_mixed(n, np.float64, 900 + n) for n in (300 * 2048 + 3, 5 * 2048, 40 * 2048 + 1)]
+    ts = [torch.from_numpy(x).cuda() for x in xs]
+    encs = [torch.zeros(api.sleek_upper_bound_size(x.nbytes), dtype=torch.uint8, device="cuda") for x in xs]
+    decs = [torch.zeros_like(t) for t in ts]
+    sizes = torch.zeros(2 * len(xs), dtype=torch.int64, device="cuda")
+
+    def calls():
+        for k, (t, e, d) in enumerate(zip(ts, encs, decs)):
+            _capi.check(L.sleek_compress_f64(t.data_ptr(), t.numel(), e.data_ptr(), sizes[2 * k:].data_ptr(),
+                                             None, 0, sh))
+            _capi.check(L.sleek_decompress_f64(e.data_ptr(), e.numel(), d.data_ptr(), t.numel() * 8,
+                                               sizes[2 * k + 1:].data_ptr(), None, 0, sh))
+
+    with torch.cuda.stream(side):
+        calls()  # outside capture: the stream's workspace exists before the capture
+    side.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=side):
+        calls()
+    want = [O.encode(x, None) for x in xs]
+    for rep in range(25):
+        for e, d in zip(encs, decs):
+            e.zero_()
+            d.zero_()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            g.replay()
+        side.synchronize()
+        for k, x in enumerate(xs):
+            n = int(sizes[2 * k].item())
+            assert encs[k][:n].cpu().numpy().tobytes() == want[k], (rep, k)
+            assert int(sizes[2 * k + 1].item()) == x.nbytes
+            assert decs[k].cpu().numpy().tobytes() == x.tobytes(), (rep, k)
+    del g
+
+
 # ---- malformed streams: an error status, never a trap ----------------------------------
 
 def test_corrupt_streams_report_status(cuda):
