@@ -613,7 +613,8 @@ __device__ __forceinline__ long long lookback(const uint64_t* flags, long long i
 // to the arbitrary global byte address `dst`.  Whole aligned 16-byte granules
 // get one vector store each, funnel-shifted from two aligned shared loads; the
 // at most two granules shared with neighbouring chunks are written byte by
-// byte.  Called by all NT threads.
+// byte.  Called by NT threads with tid = 0 .. NT-1 (the encoder: its producer
+// warp, NT = 32).
 // ----------------------------------------------------------------------------
 template <int WQ>
 __device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, int bb8)
@@ -632,9 +633,9 @@ __device__ __forceinline__ uint4 shifted_granule(const uint4 x, const uint4 y, i
 // loads hit every bank once and its stores fill whole sectors), two granules in
 // flight per thread.
 template <int WQ, int NT>
-__device__ __forceinline__ void shifted_run(uint4* out, const uint4* s4, int jf, int jl, int bb8)
+__device__ __forceinline__ void shifted_run(uint4* out, const uint4* s4, int jf, int jl, int bb8, int t)
 {
-  for (int j = jf + static_cast<int>(threadIdx.x); j < jl; j += 2 * NT) {
+  for (int j = jf + t; j < jl; j += 2 * NT) {
     const bool two = j + NT < jl;
     const uint4 x0 = s4[j - 1], y0 = s4[j];
     uint4 x1 = x0, y1 = y0;
@@ -648,9 +649,8 @@ __device__ __forceinline__ void shifted_run(uint4* out, const uint4* s4, int jf,
 }
 
 template <int NT>
-__device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len)
+__device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, int len, int tid)
 {
-  const int tid = threadIdx.x;
   const uintptr_t d = reinterpret_cast<uintptr_t>(dst);
   const int sft = static_cast<int>(d & 15u);
   uint8_t* const a0 = dst - sft;
@@ -665,10 +665,10 @@ __device__ __forceinline__ void store_shifted(uint8_t* dst, const uint8_t* src, 
     const int bo = 16 - sft;
     const int bb8 = (bo & 3) * 8;
     switch (bo >> 2) {
-      case 0: shifted_run<0, NT>(out, s4, jf, jl, bb8); break;
-      case 1: shifted_run<1, NT>(out, s4, jf, jl, bb8); break;
-      case 2: shifted_run<2, NT>(out, s4, jf, jl, bb8); break;
-      default: shifted_run<3, NT>(out, s4, jf, jl, bb8); break;
+      case 0: shifted_run<0, NT>(out, s4, jf, jl, bb8, tid); break;
+      case 1: shifted_run<1, NT>(out, s4, jf, jl, bb8, tid); break;
+      case 2: shifted_run<2, NT>(out, s4, jf, jl, bb8, tid); break;
+      default: shifted_run<3, NT>(out, s4, jf, jl, bb8, tid); break;
     }
   }
   // edge granules (shared with the neighbouring chunks): one byte per lane of

@@ -38,12 +38,12 @@ template <int CW_, int ST_, int MINB_>
 struct EncShape {
   static constexpr int CW = CW_;
   static constexpr int ST = ST_;
-  static constexpr int LAG = ST - 2;
-  static constexpr int AHEAD = ST - LAG;
+  // the copy of chunk seq is issued once the compute warps have sized chunk seq - AHEAD
+  static constexpr int AHEAD = 2;
   static constexpr int MINB = MINB_;
   static constexpr int NT = (CW + 2) * 32;  // + a producer warp and a scanner warp
   static constexpr int SPW = SC / CW;       // subchunks per compute warp
-  static_assert(SC % CW == 0 && LAG >= 1, "shape");
+  static_assert(SC % CW == 0 && AHEAD < ST, "shape");
 };
 // the shapes the library is built with (index = the C ABI's shape number)
 using EncShape0 = EncShape<8, 4, 3>;   // default: 10 warps, 66 KB, 3 CTAs per SM
@@ -72,9 +72,9 @@ struct EncMeta {
 template <int ST>
 struct EncMisc {
   uint64_t full[ST];    // chunk bytes landed (TMA tx count)
-  uint64_t empty[ST];   // go-ahead for the stage's next copy (its previous chunk is stored)
-  uint64_t sized[ST];   // compressed size of the stage's chunk known
+  uint64_t sized[ST];   // compressed size of the stage's chunk known (compute warps past phase A)
   uint64_t placed[ST];  // payload offset of the stage's chunk known
+  uint64_t packed[ST];  // every compute warp has packed its share of the stage's chunk
   EncMeta meta[ST];
   int lnv[2][SC];  // subchunk bit widths, by chunk parity (a fast warp may write the next chunk's)
 };
@@ -487,7 +487,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
 {
   constexpr int ENC_STAGES = S::ST;
   constexpr int ENC_AHEAD = S::AHEAD;
-  constexpr int ENC_LAG = S::LAG;
   constexpr int ENC_CW = S::CW;
   constexpr int ENC_NT = S::NT;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -514,9 +513,9 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
   if (tid == 0) {
     for (int s = 0; s < ENC_STAGES; ++s) {
       mbar_init(&m.full[s], 1);
-      mbar_init(&m.empty[s], ENC_CW);  // one arrival per compute warp
       mbar_init(&m.sized[s], 1);
       mbar_init(&m.placed[s], 1);
+      mbar_init(&m.packed[s], ENC_CW);  // one arrival per compute warp
     }
     mbar_fence_init();
   }
@@ -529,25 +528,46 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
   const long long total = src.total();
 
   if (warp == ENC_CW) {
-    // ===================== producer warp: tickets and TMA copies =====================
+    // ============ producer warp: tickets, TMA copies and the chunks' stores ============
     // Tickets are taken just before their chunk's copy is issued, never earlier:
     // a ticket held long before its chunk is processed makes every later chunk's
-    // look-back wait for it.
+    // look-back wait for it.  The stage's previous chunk is stored to the stream by
+    // this warp right before the stage is refilled, so the compute warps go from
+    // one chunk's pack straight to the next chunk's transform.
     unsigned long long* const tick = reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]);
+    // stores chunk q (stage q % ENC_STAGES) once it is packed and placed
+    auto store_q = [&](int q) -> bool {
+      const int sq = q % ENC_STAGES;
+      const uint32_t pq = (q / ENC_STAGES) & 1;
+      if (!mbar_wait_bounded(&m.packed[sq], pq)) return false;
+      if (!mbar_wait_bounded(&m.placed[sq], pq)) return false;
+      const EncMeta& me = m.meta[sq];
+      const long long excl = me.excl;
+      if (excl >= 0) {
+        uint8_t* const out = me.out;
+        store_shifted<32>(out + 8 + 2 * me.chunks + excl, stage0 + sq * STAGE_BYTES, me.csize, lane);
+        if (lane == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * me.c) = static_cast<uint16_t>(me.csize);
+      }
+      // the stage's generic accesses are ordered before the TMA write that refills it
+      fence_proxy_async_smem();
+      __syncwarp();
+      return true;
+    };
+    bool stored_all = true;
+    int last_seq = 0;
     unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
     unsigned issued_par = 0;  // parity of that use
     bool more = true;
     for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
-      // From seq ENC_AHEAD on, the copy for chunk seq is issued once every compute
-      // warp has finished chunk seq - ENC_AHEAD, in which the stage's previous
-      // chunk, seq - ENC_STAGES, was stored.
-      if (seq >= ENC_AHEAD) {
-        const bool ok = mbar_wait_bounded(&m.empty[s], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
-        if (__any_sync(0xffffffffu, !ok)) {
-          if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
-          break;
-        }
+      bool ok = true;
+      if (seq >= ENC_AHEAD)
+        ok = mbar_wait_bounded(&m.sized[(seq - ENC_AHEAD) % ENC_STAGES], ((seq - ENC_AHEAD) / ENC_STAGES) & 1);
+      if (ok && seq >= ENC_STAGES) ok = store_q(seq - ENC_STAGES);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+        stored_all = false;
+        break;
       }
       long long t = NO_CHUNK;
       if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
@@ -598,7 +618,16 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
           mbar_arrive(&m.full[s]);
         }
       }
+      last_seq = seq;
       if (!more) break;
+    }
+    // the chunks still in stages (seq last_seq is the end marker)
+    if (stored_all) {
+      for (int q = last_seq >= ENC_STAGES - 1 ? last_seq - ENC_STAGES + 1 : 0; q < last_seq; ++q)
+        if (!store_q(q)) {
+          if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+          break;
+        }
     }
     // never leave with a bulk copy still landing in this CTA's shared memory
     if (lane == 0) {
@@ -654,39 +683,12 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
     }
   } else {
     // ===================== compute warps =====================
-    const int cw = warp;
-    auto store = [&](int sq) {  // all compute threads; placed[] already observed
-      const int sp = sq % ENC_STAGES;
-      const EncMeta& me = m.meta[sp];
-      const long long excl = me.excl;
-      if (excl >= 0) {
-        uint8_t* const out = me.out;
-        const long long c = me.c;
-        const int csize = me.csize;
-        store_shifted<ENC_CW * 32>(out + 8 + 2 * me.chunks + excl, stage0 + sp * STAGE_BYTES, csize);
-        if (tid == 0) *reinterpret_cast<uint16_t*>(out + 8 + 2 * c) = static_cast<uint16_t>(csize);
-      }
-    };
-
-    // Each thread waits for the offset itself; a wait that gives up skips this
-    // thread's share of the store and is reported at the next barrier.
-    auto placed_store = [&](int sq) -> bool {
-      if (!mbar_wait_bounded(&m.placed[sq % ENC_STAGES], (sq / ENC_STAGES) & 1)) {
-        if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
-        return false;
-      }
-      store(sq);
-      return true;
-    };
-
     // Warps pass each other freely between the barriers of compute_chunk: each
-    // waits for its stage and its offsets itself and frees a stage with its own
-    // arrival, and the pack data one warp stores were written by the others
-    // before an earlier barrier.
-    int seq = 0;
-    bool failed = false;
+    // waits for its stage itself, and a stage goes back to the producer warp once
+    // every compute warp has packed its share of the chunk.
+    const int cw = warp;
     bool late = false;  // a wait of this thread gave up
-    for (;; ++seq) {
+    for (int seq = 0;; ++seq) {
       const int s = seq % ENC_STAGES;
       if (!mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1)) {
         if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
@@ -708,25 +710,9 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
           default: r = compute_chunk<3, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate); break;
         }
       }
-      if (r == 2) {
-        failed = true;
-        break;
-      }
-      if (r == 1) break;
-      // ---- store the chunk of seq - ENC_LAG once its offset is known -----------
-      // (waiting here rather than before the compute gives its look-back ENC_LAG
-      // chunks of compute time to finish)
-      if (seq >= ENC_LAG && !placed_store(seq - ENC_LAG)) late = true;
-      // this warp is done with the stage of seq - ENC_LAG, which the producer may
-      // now refill with chunk seq + ENC_AHEAD (generic accesses ordered before its TMA write)
-      fence_proxy_async_smem();
+      if (r != 0) break;  // end of the work (1) or a wait that gave up (2)
       __syncwarp();
-      if (lane == 0) mbar_arrive(&m.empty[(seq + ENC_AHEAD) % ENC_STAGES]);
-    }
-    if (!failed) {
-      // drain: chunks seq - ENC_LAG .. seq - 1
-      for (int q = seq >= ENC_LAG ? seq - ENC_LAG : 0; q < seq; ++q)
-        if (!placed_store(q)) break;
+      if (lane == 0) mbar_arrive(&m.packed[s]);
     }
   }
 

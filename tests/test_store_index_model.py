@@ -4,17 +4,16 @@ shared-memory address, go to an arbitrary global byte address as 16-byte stores,
 each funnel-shifted from two aligned staged granules, consecutive threads on
 consecutive granules and two granules in flight per thread, and byte stores by the
 first warp for the two granules shared with the neighbouring chunks.  The model
-repeats the kernel's index arithmetic thread by thread (the compute warps' 256
-threads) and checks, for every byte misalignment and chunk lengths from 1 byte to a
+repeats the kernel's index arithmetic thread by thread (the producer warp's 32
+threads, which store each chunk; and 256 threads, a wider caller) and checks, for every byte misalignment and chunk lengths from 1 byte to a
 full raw chunk: every destination byte is written exactly once, nothing outside the
 chunk's bytes is written, and every staged read stays inside the stage."""
 import pytest
 
 STAGE_BYTES = 16384 + 64
-NT = 256
 
 
-def model(sft, ln):
+def model(sft, ln, NT):
     a0 = 64  # a 16-byte aligned base
     dst = a0 + sft
     nunits = (sft + ln + 15) >> 4
@@ -59,10 +58,11 @@ def model(sft, ln):
 LENGTHS = list(range(1, 200)) + [255, 256, 257, 511, 512, 513, 1000, 4097, 8000, 16383 - 17, 16383, 16384]
 
 
+@pytest.mark.parametrize("nt", (32, 256))
 @pytest.mark.parametrize("sft", range(16))
-def test_store_writes_every_byte_once_and_nothing_else(sft):
+def test_store_writes_every_byte_once_and_nothing_else(sft, nt):
     for ln in LENGTHS:
-        dst, written, reads = model(sft, ln)
+        dst, written, reads = model(sft, ln, nt)
         assert all(written.get(b, 0) == 1 for b in range(dst, dst + ln)), (sft, ln)
         assert all(dst <= b < dst + ln for b in written), (sft, ln)
         assert all(0 <= g and 16 * (g + 1) <= STAGE_BYTES for g in reads), (sft, ln)
