@@ -345,30 +345,23 @@ __device__ __forceinline__ void pack_subchunks(uint32_t* pw, const int (&wbase)[
 }
 
 
-// Transform, size, publish and pack one chunk (compute warps).  KIND: bit 0 =
-// 64-bit values, bit 1 = lossy.  The barrier after phase A is the compute warps'
-// only CTA barrier per chunk and their point of agreement: every warp arrives
-// there, with `skip` (no chunk: the end, or a failed wait) and `fail` (this
-// thread's wait gave up); returns 2 if any thread failed, 1 at the end, 0 when
-// the chunk was processed.
-template <int KIND, class S>
-__device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc<S::ST>& m, uint64_t* flags, int cw,
-                                             int lane, int tid, int par, bool skip, bool fail)
-{
-  using T = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
-  constexpr bool LOSSY = (KIND & 2) != 0;
-  using V = VT<T>;
-  constexpr int P = 16 / static_cast<int>(sizeof(T));  // values per lane per subchunk
-  constexpr int SPW = S::SPW;                            // subchunks per compute warp
-  int* const lnv = m.lnv[par];
+// The per-chunk work of a compute warp, in three steps shared by both encode
+// kernels.  KIND: bit 0 = 64-bit values, bit 1 = lossy.
+template <int KIND>
+using EncVal = typename std::conditional<(KIND & 1) != 0, uint64_t, uint32_t>::type;
 
-  // ---- phase A: values into registers, transform / quantize, bit widths ------
-  // (the stage always holds a full 16 KB chunk: partial chunks are zero padded)
-  T vals[SPW][P];
-  if (!skip) {
-  const QParams q = me.q;
+// Phase A: the warp's subchunks cw, cw + CW, ... of the staged chunk into
+// registers, transformed or quantized, and their bit widths into lnv (the stage
+// always holds a full 16 KB chunk: partial chunks are zero padded).
+template <int KIND, class S>
+__device__ __forceinline__ void chunk_phase_a(const uint8_t* stg, const QParams& q, int* lnv, int cw, int lane,
+                                              EncVal<KIND> (&vals)[S::SPW][16 / sizeof(EncVal<KIND>)])
+{
+  using T = EncVal<KIND>;
+  constexpr bool LOSSY = (KIND & 2) != 0;
+  constexpr int P = 16 / static_cast<int>(sizeof(T));
 #pragma unroll
-  for (int u = 0; u < SPW; ++u) {
+  for (int u = 0; u < S::SPW; ++u) {
     const int i = cw + u * S::CW;
     const uint4 w4 = *reinterpret_cast<const uint4*>(stg + i * 512 + lane * 16);
     if constexpr (sizeof(T) == 4) {
@@ -386,43 +379,79 @@ __device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc<
     const int w = warp_bit_width(orv);
     if (lane == 0) lnv[i] = w;
   }
+}
+
+// The chunk's packed words (wtot) and its size in the stream (compressed iff
+// 34 + 4 wtot < osize), from every subchunk's width (all lanes, any warp).
+struct ChunkSize {
+  int ln;    // width of subchunk `lane`
+  int wc;    // 32-bit words of subchunk `lane`
+  int wtot;  // packed words of the chunk
+  int csize;
+  bool comp;
+};
+template <typename T>
+__device__ __forceinline__ ChunkSize chunk_size(const int* lnv, int lane, int osize)
+{
+  using V = VT<T>;
+  ChunkSize z;
+  z.ln = lnv[lane];
+  z.wc = (V::VPS * z.ln) >> 5;
+  // totals by warp reductions (independent, no shuffle-scan chain)
+  z.wtot = __reduce_add_sync(0xffffffffu, z.wc);
+  const int newsize = 34 + 4 * z.wtot;
+  z.comp = newsize < osize;
+  z.csize = z.comp ? newsize : osize;
+  return z;
+}
+
+// Packs a compressible chunk from registers to `dst` (16-byte aligned): the 32
+// width bytes, the packed words, the int16 trailer.
+template <int KIND, class S>
+__device__ __forceinline__ void chunk_pack(uint8_t* dst, const ChunkSize& z, int osize, int cw, int lane,
+                                           const EncVal<KIND> (&vals)[S::SPW][16 / sizeof(EncVal<KIND>)])
+{
+  using T = EncVal<KIND>;
+  uint32_t* const pw = reinterpret_cast<uint32_t*>(dst + 32);
+  int wbase[S::SPW], lnu[S::SPW];  // all offsets and widths first: the reductions overlap
+#pragma unroll
+  for (int u = 0; u < S::SPW; ++u) {
+    const int i = cw + u * S::CW;
+    wbase[u] = __reduce_add_sync(0xffffffffu, lane < i ? z.wc : 0);  // words of subchunks before i
+    lnu[u] = __shfl_sync(0xffffffffu, z.ln, i);
   }
+  pack_subchunks<T, S::SPW>(pw, wbase, lnu, vals, lane);
+  if (cw == 0) {
+    dst[lane] = static_cast<uint8_t>(z.ln);
+    if (lane == 0) *reinterpret_cast<int16_t*>(dst + 32 + 4 * z.wtot) = static_cast<int16_t>(osize);
+  }
+}
+
+// Transform, size, publish and pack one chunk in place (compute warps of
+// k_encode).  The barrier after phase A is the compute warps' only CTA barrier
+// per chunk and their point of agreement: every warp arrives there, with `skip`
+// (no chunk: the end, or a failed wait) and `fail` (this thread's wait gave up);
+// returns 2 if any thread failed, 1 at the end, 0 when the chunk was processed.
+template <int KIND, class S>
+__device__ __forceinline__ int compute_chunk(uint8_t* stg, EncMeta& me, EncMisc<S::ST>& m, uint64_t* flags, int cw,
+                                             int lane, int tid, int par, bool skip, bool fail)
+{
+  using T = EncVal<KIND>;
+  int* const lnv = m.lnv[par];
+  T vals[S::SPW][16 / sizeof(T)];
+  if (!skip) chunk_phase_a<KIND, S>(stg, me.q, lnv, cw, lane, vals);
   if (cbar_or<S::CW>(fail)) return 2;
   if (skip) return 1;
-
-  // ---- widths scan (every warp, redundantly), size decision -----------------
   const int osize = me.osize;
-  const int ln_l = lnv[lane];
-  const int wc = (V::VPS * ln_l) >> 5;  // 32-bit words of subchunk `lane`
-  // totals by warp reductions (independent, no shuffle-scan chain)
-  const int wtot = __reduce_add_sync(0xffffffffu, wc);
-  const int newsize = 34 + 4 * wtot;
-  const bool comp = newsize < osize;
-  const int csize = comp ? newsize : osize;
+  const ChunkSize z = chunk_size<T>(lnv, lane, osize);
   if (tid == 0) {
     const int s = static_cast<int>(&me - m.meta);
-    me.csize = csize;
-    me.comp = comp;
-    st_relaxed_u64(&flags[me.g], (me.c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(csize));
+    me.csize = z.csize;
+    me.comp = z.comp;
+    st_relaxed_u64(&flags[me.g], (me.c == 0 ? FLAG_INC : FLAG_AGG) | static_cast<uint64_t>(z.csize));
     mbar_arrive(&m.sized[s]);
   }
-
-  // ---- pack this chunk from registers ----------------------------------------
-  if (comp) {
-    uint32_t* const pw = reinterpret_cast<uint32_t*>(stg + 32);
-    int wbase[SPW], lnu[SPW];  // all offsets and widths first: the reductions overlap
-#pragma unroll
-    for (int u = 0; u < SPW; ++u) {
-      const int i = cw + u * S::CW;
-      wbase[u] = __reduce_add_sync(0xffffffffu, lane < i ? wc : 0);  // words of subchunks before i
-      lnu[u] = __shfl_sync(0xffffffffu, ln_l, i);
-    }
-    pack_subchunks<T, SPW>(pw, wbase, lnu, vals, lane);
-    if (cw == 0) {
-      stg[lane] = static_cast<uint8_t>(ln_l);
-      if (lane == 0) *reinterpret_cast<int16_t*>(stg + 32 + 4 * wtot) = static_cast<int16_t>(osize);
-    }
-  }
+  if (z.comp) chunk_pack<KIND, S>(stg, z, osize, cw, lane, vals);
   return 0;
 }
 
@@ -645,21 +674,22 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       EncMeta& me = m.meta[s];
       const long long g = me.g;
       if (g == NO_CHUNK) break;
-      // Looking back only once the chunk is sized: by then its predecessors have
-      // mostly published, so the look-back rarely polls twice.
+      // The look-back needs only the predecessors' sizes, so it starts as soon as
+      // the chunk has landed and overlaps the compute warps' phase A (measured
+      // against starting once the chunk is sized: +1-6 %).
       const long long c = me.c;
       long long excl = 0;
       unsigned err = 0;
-      ok = mbar_wait_bounded(&m.sized[s], par);
-      if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) set_status(hdr, ST_TIMEOUT, g);
-        break;
-      }
       if (c > 0) {
         excl = lookback(flags, g, me.seg, hdr);
         if (excl < 0) err = ST_TIMEOUT;
         else if (excl > c * CS) err = ST_CAPACITY;
         if (err) excl = -1;
+      }
+      ok = mbar_wait_bounded(&m.sized[s], par);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) set_status(hdr, ST_TIMEOUT, g);
+        break;
       }
       const int csize = me.csize;
       if (lane == 0) {
