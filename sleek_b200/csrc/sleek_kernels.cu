@@ -4,16 +4,18 @@
 // reference): persistent CTAs of 8 compute warps, a producer warp and a scanner
 // warp, 3 per SM.  The producer takes a chunk ticket (atomic, just in time) and
 // copies the 16 KB chunk into one of four shared-memory stages with a 1-D TMA bulk
-// copy, one chunk ahead.  Each compute warp loads 4 subchunks into registers,
+// copy, two chunks ahead.  Each compute warp loads 4 subchunks into registers,
 // transforms or quantizes them (value arithmetic restated from the reference) and
 // ORs them into bit widths; after the compute warps' one barrier per chunk every
 // warp derives the offsets it needs by warp reductions, thread 0 publishes the
-// chunk's size, and each warp packs its subchunks from registers (funnel-shifted
-// runs with one neighbour exchange; short runs by shared OR).  The scanner looks
-// back over the chunk flags and hands the payload offset to the compute warps,
-// which store the chunk two chunks later (16-byte vector stores, consecutive
-// lanes on consecutive granules).  A chunk whose encoding is not smaller than its
-// input is stored raw straight from the staged copy (never re-read from HBM).
+// chunk's size, and each warp packs its subchunks from registers into the stage
+// (funnel-shifted runs with one neighbour exchange; short runs by shared OR).  The
+// scanner looks back over the chunk flags as soon as the chunk has landed and
+// records its payload offset; the producer stores the packed chunk to the stream
+// (16-byte vector stores, consecutive lanes on consecutive granules) right before
+// it refills that stage, so the compute warps never wait for an offset.  A chunk
+// whose encoding is not smaller than its input is stored raw straight from the
+// staged copy (never re-read from HBM).
 //
 // Decode (replaces d_decode, :688-768, 1199-1279): CTAs take contiguous chunk
 // ranges in ticket order, sum their ranges' compressed sizes, look back over the
@@ -29,11 +31,10 @@ namespace sleek {
 
 // Launch shape of the encode kernel: CW compute warps (each takes SC / CW
 // subchunks of a chunk) and ST shared-memory stages of one chunk each.  The
-// compute warps store chunk k - LAG after computing chunk k (LAG = ST - 2: its
-// look-back gets LAG chunks of compute time), and the stage that store frees takes
-// chunk k + AHEAD (AHEAD = ST - LAG = 2: the producer runs one chunk ahead).
-// MINB is the CTAs per SM the registers are budgeted for.  Every shape writes the
-// same bytes.
+// producer copies chunk k once the compute warps have sized chunk k - AHEAD, right
+// after storing the stage's previous chunk, k - ST (whose look-back thereby gets
+// ST - AHEAD chunks of compute time).  MINB is the CTAs per SM the registers are
+// budgeted for.  Every shape writes the same bytes.
 template <int CW_, int ST_, int MINB_>
 struct EncShape {
   static constexpr int CW = CW_;
