@@ -444,14 +444,16 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     sizes log-uniform 1 KB - 256 MB, 60 / 40 compress / decompress, half lossy with
     bounds log-uniform in [1e-6, 1e-2], outputs in a device pool of up to 150 GB.
     Decompress requests read one of 256 distinct streams made beforehand by the
-    compressor (about 5 GB in all, many times the 126 MB L2).  The same arrival
-    trace also runs through one plain entry-point call per request (serve_plain),
-    and both forms' peaks are measured with every request queued at once.  1 % of
+    compressor (about 5 GB in all, many times the 126 MB L2).  The loop is the
+    library's native one (serve.NativeServer); the same arrival trace also runs
+    through the Python loop (serve.Server) and through one plain entry-point call
+    per request (serve_plain), and every form's peak is measured with every request
+    queued at once.  1 % of
     the served requests are re-run alone through the single-buffer entry points and
     compared bit for bit; up to 200 of them (those of at most 8 MB) are kept on the
     host for the oracle check of the CPU-baseline leg."""
     from sleek_b200 import api
-    from sleek_b200.serve import Request, Server
+    from sleek_b200.serve import NativeServer, Request, Server
 
     rng = np.random.default_rng(20261203 + 4000 + seed)
     n_src = 1 << 31  # 8 GB of f32 + 8 GB of f64 source values
@@ -495,11 +497,20 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
 
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150 << 30, free - (8 << 30)))
-    srv = Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
-    # peaks: everything queued at once, served and plain
+
+    def py_server():
+        return Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
+
+    # peaks: everything queued at once -- plain calls, the Python loop, the native loop
     warm = make(min(2000, n_requests), 0.0)
     plain_peak = serve_plain(clone(warm), dev)["gbs"]
-    peak = srv.serve(warm)["gbs"]
+    srv = py_server()
+    py_peak = srv.serve(clone(warm))["gbs"]
+    srv.close()
+    srv = None  # the arena goes back to the device before the next one
+    torch.cuda.empty_cache()
+    nat = NativeServer(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
+    peak = nat.serve(clone(warm))["gbs"]
     reqs = make(n_requests, 0.0)
     mean_bytes = np.mean([r.raw_bytes for r in reqs])
     rate = 0.7 * peak * 1e9 / mean_bytes
@@ -507,27 +518,37 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     for r in reqs:
         t += rng.exponential(1.0 / rate)
         r.arrival = t
-    plain_reqs = clone(reqs)
+    plain_reqs, py_reqs = clone(reqs), clone(reqs)
     sample = set(int(i) for i in rng.choice(len(reqs), max(1, len(reqs) // 100), replace=False))
-    stats = srv.serve(reqs, keep=lambda r: r.rid in sample)
+    stats = nat.serve(reqs, keep=lambda r: r.rid in sample)
     exact = True
     kept = []
     for r in reqs:
         if r.rid in sample:
-            got = srv.result(r)
+            got = nat.result(r)
             alone = api.compress(r.src, r.eb) if r.op == "compress" else api.decompress(r.src, r.dtype, r.eb).view(
                 torch.uint8)
             exact = exact and torch.equal(got, alone)
             if r.raw_bytes <= (8 << 20) and len(kept) < 200:
                 kept.append((r.op, r.src.cpu().numpy(), np.dtype(r.dtype), r.eb, got.cpu().numpy()))
-            srv.release(r)
+            nat.release(r)
+    got = alone = None  # views of the arena
+    nat.close()
+    nat = None
+    torch.cuda.empty_cache()
+    # the same trace through the Python loop and through plain calls
+    srv = py_server()
+    py_stats = srv.serve(py_reqs)
     srv.close()
-    del srv
+    srv = None
     torch.cuda.empty_cache()
     plain = serve_plain(plain_reqs, dev)
-    stats.update({"target_load": 0.7, "peak_gbs": peak, "arrival_rate_per_s": round(rate, 1),
+    stats.update({"loop": "native: one thread of the library admits, launches and completes (sleek_server_*)",
+                  "target_load": 0.7, "peak_gbs": peak, "arrival_rate_per_s": round(rate, 1),
                   "hbm_budget_bytes": budget, "sample_checked": len(sample), "sample_bit_exact": bool(exact),
                   "decompress_bank": {"streams": len(bank), "bytes": bank_bytes},
+                  "python_loop": {**py_stats, "peak_gbs": py_peak,
+                                  "form": "the same loop in Python (serve.Server), same trace"},
                   "plain": {**plain, "peak_gbs": plain_peak,
                             "form": "one sleek_compress_*/sleek_decompress_* call per request, one stream"},
                   "served_over_plain": {"peak": round(peak / plain_peak, 2),

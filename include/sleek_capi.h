@@ -259,6 +259,64 @@ int sleek_decompress_from_host(const unsigned char* h_encoded, long long encoded
 #define SLEEK_STREAM_SIZE_MISMATCH  7  /* the bit widths do not add up to the csize */
 #define SLEEK_STREAM_BAD_TRAILER    8  /* the trailer differs from the chunk's byte count */
 
+/* ---- Serving loop (continuous batching in a thread of the library) ---------------
+ * No counterpart in the reference, whose calls take one buffer each.  Requests are
+ * admitted once their arrival time (on the server's clock, sleek_server_now) has come
+ * and their output fits in the server's device arena (next-fit, coalescing), and run
+ * with the batched kernels on `slots` streams: an idle stream takes every admitted
+ * request waiting at that moment (at most max_batch, at most max_batch_chunks 16 KB
+ * chunks).  A request that can never run (output larger than the arena, more chunks
+ * than a launch holds) completes at once with -SLEEK_ERR_CAPACITY, and so do waiting
+ * requests when nothing on the GPU can free memory.  Results equal the single-buffer
+ * entry points' for the same request alone. */
+typedef struct sleek_server_s* sleek_server;
+
+typedef struct {
+  const void* input;        /* device: values (compress) or stream (decompress) */
+  long long num_elements;   /* compress: input elements; decompress: elements it decodes to */
+  long long stream_bytes;   /* decompress: stream length (>= 8); ignored by compress */
+  double arrival_s;         /* admitted from this time on the server's clock (<= now: at once) */
+  double error_bound;       /* lossy only */
+  long long tag;            /* the caller's id, returned with the completion */
+  int op;                   /* 0 = compress, 1 = decompress */
+  int elem_bytes;           /* 4 = float, 8 = double */
+  int lossy;                /* 0 = lossless, 1 = absolute error bound */
+  int keep;                 /* 1: the output stays in the arena until sleek_server_release */
+} sleek_server_request;
+
+typedef struct {
+  long long tag;
+  long long result_bytes;   /* bytes written (stream or values), or -status */
+  void* output;             /* kept outputs: device address in the arena; otherwise NULL */
+  double arrival_s;         /* the request's arrival time */
+  double done_s;            /* when the server saw its launch complete (server clock) */
+} sleek_server_completion;
+
+/* d_arena: device memory for the outputs (256-byte aligned; NULL = the server allocates
+ * arena_bytes itself).  Starts the server's thread and its clock. */
+int sleek_server_create(void* d_arena, long long arena_bytes, int slots, int max_batch, long long max_batch_chunks,
+                        sleek_server* server);
+int sleek_server_now(sleek_server server, double* seconds);
+/* Thread-safe; the requests' inputs must stay valid until they complete. */
+int sleek_server_submit(sleek_server server, const sleek_server_request* requests, long long n);
+/* Moves up to `capacity` completions into `out` (*n of them), waiting up to wait_ms
+ * for the first one; returns a CUDA failure of the server's own loop, if any. */
+int sleek_server_poll(sleek_server server, sleek_server_completion* out, long long capacity, long long* n,
+                      int wait_ms);
+/* Requests submitted and not yet delivered as completions (queued or in `poll`'s list). */
+int sleek_server_outstanding(sleek_server server, long long* n);
+/* The arena's free bytes as the server's loop last left them, and its size. */
+int sleek_server_arena_info(sleek_server server, long long* free_bytes, long long* size_bytes);
+/* Returns a kept output's memory to the arena. */
+int sleek_server_release(sleek_server server, void* output);
+/* Finishes every admitted request, then stops the thread and frees the server's
+ * resources (requests whose arrival time has not come are dropped). */
+int sleek_server_destroy(sleek_server server);
+/* Host-only check of the arena's policy: ops[i] > 0 allocates ops[i] bytes (offsets[i]
+ * = its offset, -1 if nothing fits); ops[i] <= 0 releases the allocation made by the
+ * (-ops[i])-th allocating op (offsets[i] = free bytes afterwards). */
+int sleek_server_arena_replay(long long arena_bytes, const long long* ops, long long n, long long* offsets);
+
 typedef struct sleek_stream_info {
   long long insize;        /* original bytes (header), -1 if unreadable */
   long long chunks;        /* chunks the header implies */

@@ -42,6 +42,17 @@ class BatchItem(C.Structure):
                 ("elem_bytes", C.c_int), ("lossy", C.c_int), ("error_bound", C.c_double)]
 
 
+class ServerRequest(C.Structure):
+    _fields_ = [("input", C.c_void_p), ("num_elements", C.c_longlong), ("stream_bytes", C.c_longlong),
+                ("arrival_s", C.c_double), ("error_bound", C.c_double), ("tag", C.c_longlong),
+                ("op", C.c_int), ("elem_bytes", C.c_int), ("lossy", C.c_int), ("keep", C.c_int)]
+
+
+class ServerCompletion(C.Structure):
+    _fields_ = [("tag", C.c_longlong), ("result_bytes", C.c_longlong), ("output", C.c_void_p),
+                ("arrival_s", C.c_double), ("done_s", C.c_double)]
+
+
 # every symbol the header declares: name -> (restype, argtypes)
 _i64 = C.c_longlong
 class StreamInfo(C.Structure):
@@ -93,6 +104,15 @@ SIGNATURES = {
     "sleek_batch_plan_destroy": (C.c_int, [_vp]),
     "sleek_compress_batch": (C.c_int, [C.c_void_p, C.c_int, _vp, _sz, _vp]),
     "sleek_decompress_batch": (C.c_int, [C.c_void_p, C.c_int, _vp, _sz, _vp]),
+    "sleek_server_create": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_void_p)]),
+    "sleek_server_now": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "sleek_server_submit": (C.c_int, [_vp, C.c_void_p, C.c_longlong]),
+    "sleek_server_poll": (C.c_int, [_vp, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong), C.c_int]),
+    "sleek_server_outstanding": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "sleek_server_arena_info": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "sleek_server_release": (C.c_int, [_vp, _vp]),
+    "sleek_server_destroy": (C.c_int, [_vp]),
+    "sleek_server_arena_replay": (C.c_int, [C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]),
 }
 
 _lib = None

@@ -18,6 +18,12 @@ arrive and run with continuous batching.
 
 Every request's result is bit-identical to running it alone through the
 single-buffer entry points (the batched kernels produce the same streams).
+
+``NativeServer`` is the same loop run by a thread of the library
+(``sleek_server_*`` in ``include/sleek_capi.h``): the whole arrival trace is
+submitted ahead with its arrival times and replayed by that thread, so no
+interpreter sits between a request's arrival, its launch and its completion;
+``Server`` keeps the loop in Python, where each step is visible.
 """
 from __future__ import annotations
 
@@ -30,6 +36,7 @@ import numpy as np
 import torch
 
 from . import _capi
+from ._capi import C
 from .api import sleek_upper_bound_size
 
 GRANULE = 256
@@ -37,6 +44,11 @@ ITEM_DTYPE = np.dtype([("input", np.uint64), ("output", np.uint64), ("size_out",
                        ("num_elements", np.int64), ("stream_bytes", np.int64), ("elem_bytes", np.int32),
                        ("lossy", np.int32), ("error_bound", np.float64)])
 assert ITEM_DTYPE.itemsize == 56  # sleek_batch_item
+SERVER_REQUEST_DTYPE = np.dtype([("input", np.uint64), ("num_elements", np.int64), ("stream_bytes", np.int64),
+                                 ("arrival_s", np.float64), ("error_bound", np.float64), ("tag", np.int64),
+                                 ("op", np.int32), ("elem_bytes", np.int32), ("lossy", np.int32),
+                                 ("keep", np.int32)])
+assert SERVER_REQUEST_DTYPE.itemsize == 64  # sleek_server_request
 
 
 class DevicePool:
@@ -301,13 +313,7 @@ class Server:
         return self.stats()
 
     def stats(self) -> dict:
-        lat = np.array([r.done - r.arrival for r in self.completed]) * 1e3
-        span = max(r.done for r in self.completed) - min(r.arrival for r in self.completed)
-        nbytes = sum(r.raw_bytes for r in self.completed)
-        return {"requests": len(self.completed), "bytes": nbytes, "span_s": round(span, 4),
-                "gbs": round(nbytes / span / 1e9, 1) if span > 0 else None,
-                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                "errors": sum(1 for r in self.completed if r.result_bytes < 0)}
+        return _stats(self.completed)
 
     def close(self) -> None:
         for s in self.slots:
@@ -315,6 +321,112 @@ class Server:
             for h in s.plans.values():
                 self._L.sleek_batch_plan_destroy(h)
             s.plans = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stats(completed: List[Request]) -> dict:
+    lat = np.array([r.done - r.arrival for r in completed]) * 1e3
+    span = max(r.done for r in completed) - min(r.arrival for r in completed)
+    nbytes = sum(r.raw_bytes for r in completed)
+    return {"requests": len(completed), "bytes": nbytes, "span_s": round(span, 4),
+            "gbs": round(nbytes / span / 1e9, 1) if span > 0 else None,
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "errors": sum(1 for r in completed if r.result_bytes < 0)}
+
+
+class NativeServer:
+    """The serving loop of ``Server`` run by a thread of the library: requests are
+    admitted at their arrival times on the server's clock when their output fits in
+    the arena (a device tensor owned here), launched with the batched kernels on
+    ``slots`` streams, and completed when the library's thread sees their launch
+    finish.  Same results, same admission rules, same statistics as ``Server``."""
+
+    def __init__(self, hbm_budget: int, slots: int = 4, max_batch: int = 512, max_batch_chunks: int = 1 << 16,
+                 device="cuda"):
+        self.arena = torch.empty((hbm_budget // GRANULE) * GRANULE, dtype=torch.uint8, device=device)
+        self.base = self.arena.data_ptr()
+        self._L = _capi.lib()
+        h = C.c_void_p()
+        _capi.check(self._L.sleek_server_create(self.base, self.arena.numel(), slots, max_batch, max_batch_chunks,
+                                                C.byref(h)), "sleek_server_create")
+        self._h = h
+        self.completed: List[Request] = []
+
+    def now(self) -> float:
+        t = C.c_double()
+        _capi.check(self._L.sleek_server_now(self._h, C.byref(t)))
+        return t.value
+
+    def arena_info(self):
+        """(free bytes, size) of the arena."""
+        f, n = C.c_longlong(), C.c_longlong()
+        _capi.check(self._L.sleek_server_arena_info(self._h, C.byref(f), C.byref(n)))
+        return f.value, n.value
+
+    def serve(self, requests: List[Request], keep=None, lead_s: float = 0.02) -> dict:
+        """Submits the requests with their arrival times (seconds from now, plus a
+        lead for the submission itself) and waits for all of them.  Outputs
+        are returned to the arena on completion unless ``keep(r)`` is true."""
+        n = len(requests)
+        arr = np.zeros(max(n, 1), SERVER_REQUEST_DTYPE)
+        comp = np.array([r.op == "compress" for r in requests], dtype=bool)
+        arr["input"][:n] = [r.src.data_ptr() for r in requests]
+        arr["num_elements"][:n] = [r.src.numel() if c else r.num_elements for r, c in zip(requests, comp)]
+        arr["stream_bytes"][:n] = [0 if c else r.src.numel() for r, c in zip(requests, comp)]
+        arr["error_bound"][:n] = [float(r.eb) if r.eb is not None else 0.0 for r in requests]
+        arr["tag"][:n] = np.arange(n)
+        arr["op"][:n] = np.where(comp, 0, 1)
+        arr["elem_bytes"][:n] = [np.dtype(r.dtype).itemsize for r in requests]
+        arr["lossy"][:n] = [int(r.eb is not None) for r in requests]
+        arr["keep"][:n] = [int(keep is not None and bool(keep(r))) for r in requests]
+        rel = np.array([r.arrival for r in requests], dtype=np.float64)
+        # arrivals on the server's clock, set once the array is built; the lead
+        # covers the submission and the loop taking the requests in (a few
+        # hundred ns per request)
+        t0 = self.now() + lead_s + 5e-7 * n
+        arr["arrival_s"][:n] = t0 + rel
+        _capi.check(self._L.sleek_server_submit(self._h, arr.ctypes.data, n), "sleek_server_submit")
+        buf = (_capi.ServerCompletion * 4096)()
+        got = C.c_longlong()
+        completed = []
+        while len(completed) < n:
+            _capi.check(self._L.sleek_server_poll(self._h, buf, len(buf), C.byref(got), 100), "sleek_server_poll")
+            for k in range(got.value):
+                c = buf[k]
+                r = requests[c.tag]
+                r.done = c.done_s - t0
+                r.result_bytes = c.result_bytes
+                r.out_off = (c.output - self.base) if c.output else -1
+                r.out_bytes = max(c.result_bytes, 0)
+                completed.append(r)
+        self.completed = completed
+        return self.stats()
+
+    def result(self, r: Request) -> torch.Tensor:
+        """A completed, kept request's output (a view into the arena until released)."""
+        if r.result_bytes < 0:
+            raise _capi.SleekError(-r.result_bytes, "serve")
+        if r.out_off < 0:
+            raise ValueError("the request's output was not kept")
+        return self.arena[r.out_off:r.out_off + r.result_bytes]
+
+    def release(self, r: Request) -> None:
+        if r.out_off >= 0:
+            _capi.check(self._L.sleek_server_release(self._h, C.c_void_p(self.base + r.out_off)))
+            r.out_off = -1
+
+    def stats(self) -> dict:
+        return _stats(self.completed)
+
+    def close(self) -> None:
+        if self._h is not None:
+            _capi.check(self._L.sleek_server_destroy(self._h), "sleek_server_destroy")
+            self._h = None
 
     def __del__(self):
         try:

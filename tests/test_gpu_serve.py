@@ -1,14 +1,18 @@
 """The serving loop (continuous batching over several streams, outputs in a
-device pool admitted by free memory): every request's result is bit-identical to
-the same request run alone through the single-buffer entry points, and the loop
-reports latency percentiles and throughput."""
+device pool admitted by free memory), in Python (Server) and in a thread of the
+library (NativeServer): every request's result is bit-identical to the same
+request run alone through the single-buffer entry points, and the loop reports
+latency percentiles and throughput."""
+import time
+
 import numpy as np
 import pytest
 import torch
 
 from oracle import oracle as O
 from sleek_b200 import api
-from sleek_b200.serve import Request, Server
+from sleek_b200 import _capi
+from sleek_b200.serve import NativeServer, Request, Server
 
 pytestmark = pytest.mark.gpu
 
@@ -80,4 +84,81 @@ def test_serving_sample_matches_oracle(cuda):
         else:
             assert got == O.decode(r.src.cpu().numpy().tobytes(), r.dtype, r.eb).tobytes()
         srv.release(r)
+    srv.close()
+
+
+def _alone(r):
+    if r.op == "compress":
+        return api.compress(r.src, r.eb)
+    return api.decompress(r.src, r.dtype, r.eb).view(torch.uint8)
+
+
+def test_native_serving_results_equal_alone_runs(cuda):
+    reqs = _requests(300, 1)
+    srv = NativeServer(hbm_budget=2 << 30, slots=3, max_batch=64)
+    stats = srv.serve(reqs, keep=lambda r: True)
+    assert stats["requests"] == len(reqs) and stats["errors"] == 0
+    assert stats["p50_ms"] > 0 and stats["p99_ms"] >= stats["p50_ms"]
+    assert all(r.done >= r.arrival for r in reqs)
+    for r in reqs:
+        assert torch.equal(srv.result(r), _alone(r)), (r.rid, r.op)
+        srv.release(r)
+    torch.cuda.synchronize()
+    for _ in range(100):  # the loop applies releases on its next pass
+        free, size = srv.arena_info()
+        if free == size:
+            break
+        time.sleep(0.01)
+    assert free == size
+    srv.close()
+
+
+def test_native_serving_admits_by_free_memory(cuda):
+    # an arena that holds only a few outputs at a time: everything still completes
+    reqs = _requests(60, 2)
+    srv = NativeServer(hbm_budget=64 << 20, slots=2, max_batch=16)
+    stats = srv.serve(reqs)
+    assert stats["requests"] == len(reqs) and stats["errors"] == 0
+    srv.close()
+
+
+def test_native_serving_sample_matches_oracle(cuda):
+    reqs = [r for r in _requests(40, 3) if r.raw_bytes < (1 << 20)][:10]
+    srv = NativeServer(hbm_budget=1 << 30, slots=2, max_batch=8)
+    srv.serve(reqs, keep=lambda r: True)
+    for r in reqs:
+        got = srv.result(r).cpu().numpy().tobytes()
+        if r.op == "compress":
+            assert got == O.encode(r.src.cpu().numpy(), r.eb)
+        else:
+            assert got == O.decode(r.src.cpu().numpy().tobytes(), r.dtype, r.eb).tobytes()
+        srv.release(r)
+    srv.close()
+
+
+def test_native_serving_fails_impossible_requests_at_once(cuda):
+    x = torch.zeros(3 << 20, dtype=torch.float32, device="cuda")  # 12 MB, output larger than the arena
+    small = torch.zeros(1000, dtype=torch.float32, device="cuda")
+    reqs = [Request("compress", x, np.dtype(np.float32), None, arrival=0.0, rid=0),
+            Request("compress", small, np.dtype(np.float32), None, arrival=0.0, rid=1)]
+    srv = NativeServer(hbm_budget=8 << 20, slots=1, max_batch=4)
+    stats = srv.serve(reqs, keep=lambda r: True)
+    assert stats["requests"] == 2 and stats["errors"] == 1
+    assert reqs[0].result_bytes == -_capi.SLEEK_ERR_CAPACITY
+    assert torch.equal(srv.result(reqs[1]), api.compress(small, None))
+    srv.release(reqs[1])
+    srv.close()
+
+
+def test_native_serving_replays_arrival_times(cuda):
+    # requests spaced 20 ms apart are not completed before they arrive
+    src = torch.cumsum(torch.randn(1 << 16, device="cuda"), 0)
+    reqs = [Request("compress", src, np.dtype(np.float32), 1e-3, arrival=0.02 * k, rid=k) for k in range(5)]
+    srv = NativeServer(hbm_budget=256 << 20, slots=2, max_batch=8)
+    stats = srv.serve(reqs)
+    assert stats["errors"] == 0
+    for r in reqs:
+        assert r.done >= r.arrival
+        assert r.done - r.arrival < 0.015  # served alone, promptly
+    assert stats["span_s"] >= 0.08
     srv.close()
