@@ -928,7 +928,12 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       mbar_init(&m.empty[st], NW);  // one arrival per warp
     }
     mbar_fence_init();
-    m.vb = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]), 1ull));
+    // ranges placed by summing the size table wait on no other CTA, so the
+    // block index orders them; the look-back needs ticket order (a CTA waits only
+    // on CTAs that started before it)
+    m.vb = hdr_ok && cap_ok && chunks <= DEC_DIRECT_MAX
+               ? static_cast<long long>(blockIdx.x)
+               : static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]), 1ull));
     if (!hdr_ok) set_status(hdr, ST_CORRUPT, -1);
     else if (!cap_ok) set_status(hdr, ST_CAPACITY, -1);
   }
