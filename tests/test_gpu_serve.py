@@ -162,3 +162,67 @@ def test_native_serving_replays_arrival_times(cuda):
         assert r.done - r.arrival < 0.015  # served alone, promptly
     assert stats["span_s"] >= 0.08
     srv.close()
+
+
+
+def _native_requests(xs, tag0):
+    arr = (_capi.ServerRequest * len(xs))()
+    for i, x in enumerate(xs):
+        q = arr[i]
+        q.input = x.data_ptr()
+        q.num_elements = x.numel()
+        q.tag = tag0 + i
+        q.op = 0
+        q.elem_bytes = 4
+        q.keep = 1
+    return arr
+
+
+def _drain(srv, n):
+    L = _capi.lib()
+    buf = (_capi.ServerCompletion * 256)()
+    got, k = {}, _capi.C.c_longlong()
+    while len(got) < n:
+        _capi.check(L.sleek_server_poll(srv._h, buf, 256, _capi.C.byref(k), 200))
+        for i in range(k.value):
+            got[buf[i].tag] = (buf[i].result_bytes, buf[i].output)
+    return got
+
+
+def test_native_server_takes_requests_from_several_threads(cuda):
+    import threading
+
+    L = _capi.lib()
+    srv = NativeServer(hbm_budget=1 << 30, slots=3, max_batch=32, max_batch_chunks=1 << 14)
+    src = torch.cumsum(torch.randn(1 << 22, device="cuda"), 0) * 0.01
+    groups = [[src[k * 1000 + j * 7: k * 1000 + j * 7 + 5000 + 300 * j] for j in range(40)] for k in range(4)]
+    arrays = [_native_requests(g, 1000 * k) for k, g in enumerate(groups)]
+    ths = [threading.Thread(target=lambda a=a: _capi.check(L.sleek_server_submit(srv._h, a, len(a))))
+           for a in arrays]
+    [t.start() for t in ths]
+    [t.join() for t in ths]
+    got = _drain(srv, 160)
+    for k, g in enumerate(groups):
+        for i, x in enumerate(g):
+            res, ptr = got[1000 * k + i]
+            off = ptr - srv.base
+            assert torch.equal(srv.arena[off:off + res], api.compress(x, None))
+            assert L.sleek_server_release(srv._h, _capi.C.c_void_p(ptr)) == 0
+    n = _capi.C.c_longlong()
+    _capi.check(L.sleek_server_outstanding(srv._h, _capi.C.byref(n)))
+    assert n.value == 0
+    srv.close()
+
+
+def test_native_server_destroy_with_launches_in_flight(cuda):
+    # destroy finishes what was admitted and returns; releases of unknown
+    # addresses are ignored
+    L = _capi.lib()
+    srv = NativeServer(hbm_budget=4 << 30, slots=2, max_batch=16)
+    src = torch.cumsum(torch.randn(1 << 26, device="cuda"), 0) * 0.01
+    xs = [src[j << 20: (j << 20) + (8 << 20)] for j in range(20)]
+    a = _native_requests(xs, 0)
+    _capi.check(L.sleek_server_submit(srv._h, a, len(a)))
+    assert L.sleek_server_release(srv._h, _capi.C.c_void_p(srv.base + 12345 * 256)) == 0
+    srv.close()  # returns once the admitted work is done
+    torch.cuda.synchronize()
