@@ -350,19 +350,26 @@ void loop(sleek_server_s* s)
         s->queue.push_back(std::move(q));
     }
 
-    // dispatch to idle slots
-    for (Slot& sl : s->slots) {
-      if (s->queue.empty()) break;
-      if (sl.busy) continue;
-      std::vector<Req> reqs = take(s);
-      if (reqs.empty()) break;
-      if (launch(s, sl, reqs, out) != SLEEK_OK) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->error = SLEEK_ERR_CUDA;
-      }
-    }
+    // dispatch to idle slots (again after a launch that failed: it returned its
+    // requests' memory, which may admit others)
     bool busy = false;
-    for (const Slot& sl : s->slots) busy = busy || sl.busy;
+    for (bool retry = true; retry;) {
+      retry = false;
+      for (Slot& sl : s->slots) {
+        if (s->queue.empty()) break;
+        if (sl.busy) continue;
+        std::vector<Req> reqs = take(s);
+        if (reqs.empty()) break;
+        if (launch(s, sl, reqs, out) != SLEEK_OK) {
+          std::lock_guard<std::mutex> lk(s->mu);
+          s->error = SLEEK_ERR_CUDA;
+        }
+        if (!sl.busy) retry = true;
+      }
+      busy = false;
+      for (const Slot& sl : s->slots) busy = busy || sl.busy;
+      retry = retry && !busy && !s->queue.empty();
+    }
     if (!s->queue.empty() && !busy) {
       // nothing on the GPU can free memory: what waits cannot be admitted
       const double tf = s->now();
@@ -383,7 +390,14 @@ void loop(sleek_server_s* s)
       if (!s->incoming.empty() || !s->releases.empty() || s->stop) continue;
       double wait = 1e-3;
       if (!s->pending.empty()) wait = std::min(wait, std::max(0.0, s->pending.front().r.arrival_s - s->now()));
-      if (wait > 0) s->cv_in.wait_for(lk, std::chrono::duration<double>(wait));
+      // a timed wait overshoots by tens of microseconds: arrivals that close are
+      // waited for by yielding
+      if (wait < 200e-6) {
+        lk.unlock();
+        std::this_thread::yield();
+        continue;
+      }
+      s->cv_in.wait_for(lk, std::chrono::duration<double>(wait - 100e-6));
     }
   }
 }
