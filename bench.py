@@ -497,12 +497,13 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
 
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150 << 30, free - (8 << 30)))
-    # a launch holds at most 16,384 chunks (256 MB, the largest request): a batch
-    # completes as a whole, so smaller batches shorten the tail (p99 1.1 -> 0.9 ms
-    # against 2 GB batches at this load)
+    # launches of up to 131,072 chunks (2 GB): capping them at the largest request
+    # (256 MB) shortens the native loop's tail at equal load (p99 1.1 -> 0.9 ms)
+    # but lowers its peak by 12 % and starves the Python loop, whose cost per
+    # launch then dominates
 
     def py_server():
-        return Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 14)
+        return Server(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
 
     # peaks: everything queued at once -- plain calls, the Python loop, the native loop
     warm = make(min(2000, n_requests), 0.0)
@@ -512,7 +513,7 @@ def bench_serve(dev, n_requests: int, seed: int = 4):
     srv.close()
     srv = None  # the arena goes back to the device before the next one
     torch.cuda.empty_cache()
-    nat = NativeServer(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 14)
+    nat = NativeServer(hbm_budget=budget, slots=4, max_batch=512, max_batch_chunks=1 << 17)
     peak = nat.serve(clone(warm))["gbs"]
     reqs = make(n_requests, 0.0)
     mean_bytes = np.mean([r.raw_bytes for r in reqs])
