@@ -241,6 +241,44 @@ def test_library_workspace_resets_itself_between_calls(cuda):
         assert status.value == _capi.SLEEK_OK
 
 
+def test_concurrent_streams_keep_their_own_workspaces(cuda):
+    # Three streams, each with its library-owned workspace, take turns enqueueing
+    # compress and decompress calls of different sizes and kinds with no host wait
+    # in between; every stream and decoded array equals the oracle's.
+    from sleek_b200 import _capi
+    L = _capi.lib()
+    streams = [torch.cuda.Stream() for _ in range(3)]
+    jobs = []
+    for k in range(12):
+        dt = np.float32 if k % 2 else np.float64
+        eb = None if k % 3 == 0 else (1e-3 if k % 3 == 1 else 1e-5)
+        x = _mixed(int(30000 + 45000 * (k % 5)) + k, dt, 900 + k)
+        t = torch.from_numpy(x).cuda()
+        n = x.size * x.itemsize
+        enc = torch.zeros(api.sleek_upper_bound_size(n), dtype=torch.uint8, device="cuda")
+        dec = torch.zeros_like(t)
+        sizes = torch.zeros(2, dtype=torch.int64, device="cuda")
+        jobs.append((x, eb, t, enc, dec, sizes))
+    torch.cuda.synchronize()
+    w = lambda dt: "f32" if dt == np.float32 else "f64"
+    for k, (x, eb, t, enc, dec, sizes) in enumerate(jobs):
+        sh = streams[k % 3].cuda_stream
+        pre = (api.sleek_error_bound(eb, x.dtype).c_struct(),) if eb is not None else ()
+        mid = "_lossy" if eb is not None else ""
+        _capi.check(getattr(L, f"sleek_compress{mid}_{w(x.dtype)}")(
+            *pre, t.data_ptr(), t.numel(), enc.data_ptr(), sizes.data_ptr(), None, 0, sh))
+        _capi.check(getattr(L, f"sleek_decompress{mid}_{w(x.dtype)}")(
+            *pre, enc.data_ptr(), enc.numel(), dec.data_ptr(), t.numel() * x.itemsize, sizes[1:].data_ptr(),
+            None, 0, sh))
+    torch.cuda.synchronize()
+    for x, eb, t, enc, dec, sizes in jobs:
+        want = O.encode(x, eb)
+        assert int(sizes[0]) == len(want)
+        assert enc[:len(want)].cpu().numpy().tobytes() == want
+        assert int(sizes[1]) == x.size * x.itemsize
+        assert dec.cpu().numpy().tobytes() == O.decode(want, x.dtype, eb).tobytes()
+
+
 def test_graph_replays_with_the_library_workspace(cuda):
     # Captured calls keep their workspace pointer; the workspace's epoch lives on the
     # device, so replaying the graph many times (encodes and decodes of different
