@@ -909,8 +909,33 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   const WsPhase ph = WsPhase::of(a.ws, a.flag_cap);  // self-resetting workspace
   uint64_t* const hdr = ph.hdr;
   uint64_t* const flags = ph.flags;
-  // this CTA's share of the flags the previous launch left in the other region
-  if (warp == NW - 1) ph.clear_other_share(lane);
+
+  // Speculation: when the caller states the output capacity and the stream's
+  // length, the chunk count is usually ceil(capacity / CS), and this CTA's sizes
+  // (the prefix before its range, and its range) are read while the header is
+  // still on its way, instead of one dependent round trip after it.  Used only if
+  // the header agrees; the reads stay inside the stated stream length.
+  const long long g_chunks = a.out_cap > 0 ? (a.out_cap + CS - 1) / CS : -1;
+  const bool spec = g_chunks > 0 && g_chunks <= DEC_DIRECT_MAX && a.in_len >= 8 + 2 * g_chunks;
+  long long s_pre = 0;  // this thread's share of the sizes before the range
+  int s_cs = -1;        // this thread's size in the range (ranges of at most NT chunks)
+  {
+    const uint16_t* const sz = reinterpret_cast<const uint16_t*>(a.in + 8);
+    if (spec) {
+      const long long kg = (g_chunks + gridDim.x - 1) / gridDim.x;
+      const long long c0g = min(static_cast<long long>(blockIdx.x) * kg, g_chunks);
+      const long long c1g = min(c0g + kg, g_chunks);
+      if (kg <= NT && c0g + tid < c1g) s_cs = sz[c0g + tid];
+      const unsigned long long* const s8 = reinterpret_cast<const unsigned long long*>(sz);
+      const long long q = c0g >> 2;
+      for (long long k = tid; k < q; k += NT) {
+        const unsigned long long v = s8[k];
+        const unsigned long long p2 = (v & 0x0000ffff0000ffffull) + ((v >> 16) & 0x0000ffff0000ffffull);
+        s_pre += static_cast<long long>((p2 & 0xffffffffull) + (p2 >> 32));
+      }
+      for (long long c = (q << 2) + tid; c < c0g; c += NT) s_pre += sz[c];
+    }
+  }
 
   // header checks (every CTA reads the 8-byte header)
   const long long insize = *reinterpret_cast<const long long*>(a.in);
@@ -948,15 +973,28 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
   // ---- range aggregate + size-table validation ---------------------------------
   {
     const bool direct = go && chunks <= DEC_DIRECT_MAX;
+    const bool hit = direct && spec && chunks == g_chunks;  // the speculative reads are this CTA's
     long long sum = 0, pre = 0;
     int bad = 0;
-    for (long long c = c0 + tid; c < c1; c += NT) {
-      const int cs = size_in[c];
-      const int os = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
-      bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
-      sum += cs;
+    if (hit && K <= NT) {
+      if (c0 + tid < c1) {
+        const int cs = s_cs;
+        const long long c = c0 + tid;
+        const int os = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+        bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
+        sum += cs;
+      }
+    } else {
+      for (long long c = c0 + tid; c < c1; c += NT) {
+        const int cs = size_in[c];
+        const int os = static_cast<int>(min(static_cast<long long>(CS), insize - c * CS));
+        bad |= (cs > os) | (cs == 0) | ((cs < os) & (cs < 34));
+        sum += cs;
+      }
     }
-    if (direct) {
+    if (hit) {
+      pre = warp_sum(s_pre);
+    } else if (direct) {
       // sizes [0, c0), four per 8-byte load (the table starts 8-byte aligned)
       const unsigned long long* const s8 = reinterpret_cast<const unsigned long long*>(size_in);
       const long long q = c0 >> 2;
@@ -1101,6 +1139,10 @@ __global__ void __launch_bounds__(NT, MINB) k_decode(const DecArgs a)
       }
     }
   }
+
+  // this CTA's share of the flags the previous launch left in the other region
+  // (off the start of the kernel: only the next launch reads them)
+  if (warp == NW - 1) ph.clear_other_share(lane);
 
   // ---- epilogue ------------------------------------------------------------------
   __syncthreads();
