@@ -251,6 +251,15 @@ int launch(sleek_server_s* s, Slot& sl, std::vector<Req>& reqs, std::vector<slee
   if (cudaMemcpyAsync(sl.h_sizes, sl.d_sizes, sizeof(long long) * k, cudaMemcpyDeviceToHost, sl.st) != cudaSuccess ||
       cudaEventRecord(sl.ev, sl.st) != cudaSuccess) {
     cudaGetLastError();
+    // the launch cannot be completed by its event: its requests fail now (their
+    // memory is returned once the stream has finished with it)
+    cudaStreamSynchronize(sl.st);
+    cudaGetLastError();
+    const double t = s->now();
+    for (const Req& q : ok) {
+      s->arena.release(q.off, q.out_bytes);
+      failed.push_back(completion_of(q, -SLEEK_ERR_CUDA, nullptr, t));
+    }
     return SLEEK_ERR_CUDA;
   }
   sl.reqs = std::move(ok);
