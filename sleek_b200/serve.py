@@ -28,6 +28,7 @@ interpreter sits between a request's arrival, its launch and its completion;
 from __future__ import annotations
 
 import bisect
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import List, Optional
@@ -356,6 +357,7 @@ class NativeServer:
                                                 C.byref(h)), "sleek_server_create")
         self._h = h
         self.completed: List[Request] = []
+        self._serving = threading.Lock()  # serve() tags requests by position: one call at a time
 
     def now(self) -> float:
         t = C.c_double()
@@ -371,7 +373,13 @@ class NativeServer:
     def serve(self, requests: List[Request], keep=None, lead_s: float = 0.02) -> dict:
         """Submits the requests with their arrival times (seconds from now, plus a
         lead for the submission itself) and waits for all of them.  Outputs
-        are returned to the arena on completion unless ``keep(r)`` is true."""
+        are returned to the arena on completion unless ``keep(r)`` is true.  Calls
+        from several threads run one after the other (the C ABI itself takes
+        submissions from any thread)."""
+        with self._serving:
+            return self._serve(requests, keep, lead_s)
+
+    def _serve(self, requests: List[Request], keep, lead_s: float) -> dict:
         n = len(requests)
         arr = np.zeros(max(n, 1), SERVER_REQUEST_DTYPE)
         comp = np.array([r.op == "compress" for r in requests], dtype=bool)
