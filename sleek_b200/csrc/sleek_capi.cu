@@ -24,7 +24,7 @@ constexpr int WS_BLOCK = 8;
 constexpr int WS_EPOCH = 16;
 constexpr int WS_MINMAX = 24;
 
-constexpr int SHAPES_MAX = 4;
+constexpr int SHAPES_MAX = 8;
 constexpr int BUCKETS = 64;  // input sizes by their base-2 logarithm
 
 // what the single-buffer calls of one kind launch for one size bucket

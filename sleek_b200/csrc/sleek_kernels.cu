@@ -50,7 +50,9 @@ struct EncShape {
 using EncShape0 = EncShape<8, 4, 3>;   // default: 10 warps, 66 KB, 3 CTAs per SM
 using EncShape1 = EncShape<16, 4, 2>;  // 18 warps, 66 KB, 2 CTAs per SM
 using EncShape2 = EncShape<4, 4, 3>;   // 6 warps, 66 KB, 3 CTAs per SM
-constexpr int ENC_SHAPES = 3;
+using EncShape3 = EncShape<8, 3, 3>;   // 10 warps, 3 stages (50 KB), 3 CTAs per SM
+using EncShape4 = EncShape<8, 5, 2>;   // 10 warps, 5 stages (83 KB), 2 CTAs per SM
+constexpr int ENC_SHAPES = 5;
 constexpr long long NO_CHUNK = 0x7fffffffffffffffll;
 
 // What the producer tells the compute and scanner warps about the chunk in a stage.
@@ -1470,6 +1472,8 @@ static cudaError_t launch_enc_kind(int shape, const EncArgs& a, int grid, cudaSt
   switch (shape) {
     case 1: return launch_enc_k<KIND, EncShape1>(a, grid, st);
     case 2: return launch_enc_k<KIND, EncShape2>(a, grid, st);
+    case 3: return launch_enc_k<KIND, EncShape3>(a, grid, st);
+    case 4: return launch_enc_k<KIND, EncShape4>(a, grid, st);
     default: return launch_enc_k<KIND, EncShape0>(a, grid, st);
   }
 }
@@ -1480,6 +1484,8 @@ static int enc_occupancy_kind(int shape)
   switch (shape) {
     case 1: return enc_occupancy<KIND, EncShape1>();
     case 2: return enc_occupancy<KIND, EncShape2>();
+    case 3: return enc_occupancy<KIND, EncShape3>();
+    case 4: return enc_occupancy<KIND, EncShape4>();
     default: return enc_occupancy<KIND, EncShape0>();
   }
 }
@@ -1534,6 +1540,8 @@ ShapeInfo shape_info(bool enc, int shape)
     switch (shape) {
       case 1: r = {EncShape1::NT, EncShape1::CW, EncShape1::ST, EncShape1::MINB}; break;
       case 2: r = {EncShape2::NT, EncShape2::CW, EncShape2::ST, EncShape2::MINB}; break;
+      case 3: r = {EncShape3::NT, EncShape3::CW, EncShape3::ST, EncShape3::MINB}; break;
+      case 4: r = {EncShape4::NT, EncShape4::CW, EncShape4::ST, EncShape4::MINB}; break;
       default: r = {EncShape0::NT, EncShape0::CW, EncShape0::ST, EncShape0::MINB}; break;
     }
   } else {
