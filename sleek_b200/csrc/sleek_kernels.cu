@@ -585,7 +585,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       __syncwarp();
       return true;
     };
-    bool stored_all = true;
     int last_seq = 0;
     unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
     unsigned issued_par = 0;  // parity of that use
@@ -598,7 +597,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       if (ok && seq >= ENC_STAGES) ok = store_q(seq - ENC_STAGES);
       if (__any_sync(0xffffffffu, !ok)) {
         if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
-        stored_all = false;
         break;
       }
       long long t = NO_CHUNK;
@@ -653,14 +651,8 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       last_seq = seq;
       if (!more) break;
     }
-    // the chunks still in stages (seq last_seq is the end marker)
-    if (stored_all) {
-      for (int q = last_seq >= ENC_STAGES - 1 ? last_seq - ENC_STAGES + 1 : 0; q < last_seq; ++q)
-        if (!store_q(q)) {
-          if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
-          break;
-        }
-    }
+    // (the chunks still in stages, the last ENC_STAGES - 1, are stored by the
+    // compute warps, idle by then: eight warps instead of one at the kernel's end)
     // never leave with a bulk copy still landing in this CTA's shared memory
     if (lane == 0) {
       for (int s = 0; s < ENC_STAGES; ++s)
@@ -721,7 +713,9 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
     // every compute warp has packed its share of the chunk.
     const int cw = warp;
     bool late = false;  // a wait of this thread gave up
-    for (int seq = 0;; ++seq) {
+    int seq = 0;
+    int r = 0;
+    for (;; ++seq) {
       const int s = seq % ENC_STAGES;
       if (!mbar_wait_bounded(&m.full[s], (seq / ENC_STAGES) & 1)) {
         if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
@@ -732,7 +726,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       const bool wlate = __any_sync(0xffffffffu, late);
       const bool skip = wlate || me.g == NO_CHUNK;
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
-      int r;
       if constexpr (KIND >= 0) {
         r = compute_chunk<KIND, S>(stg, me, m, flags, cw, lane, tid, seq & 1, skip, wlate);
       } else {
@@ -746,6 +739,24 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       if (r != 0) break;  // end of the work (1) or a wait that gave up (2)
       __syncwarp();
       if (lane == 0) mbar_arrive(&m.packed[s]);
+    }
+    if (r == 1) {
+      // The producer stored chunks 0 .. seq - ENC_STAGES as it refilled their
+      // stages (seq is the end marker); the rest, packed before the end's
+      // barrier, are stored here once placed.
+      for (int q = seq >= ENC_STAGES - 1 ? seq - ENC_STAGES + 1 : 0; q < seq; ++q) {
+        const int sq = q % ENC_STAGES;
+        if (!mbar_wait_bounded(&m.placed[sq], (q / ENC_STAGES) & 1)) {
+          if (lane == 0) set_status(hdr, ST_TIMEOUT, -1);
+          continue;
+        }
+        const EncMeta& me = m.meta[sq];
+        const long long excl = me.excl;
+        if (excl >= 0) {
+          store_shifted<ENC_CW * 32>(me.out + 8 + 2 * me.chunks + excl, stage0 + sq * STAGE_BYTES, me.csize, tid);
+          if (tid == 0) *reinterpret_cast<uint16_t*>(me.out + 8 + 2 * me.c) = static_cast<uint16_t>(me.csize);
+        }
+      }
     }
   }
 

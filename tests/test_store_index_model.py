@@ -5,7 +5,8 @@ each funnel-shifted from two aligned staged granules, consecutive threads on
 consecutive granules and two granules in flight per thread, and byte stores by the
 first warp for the two granules shared with the neighbouring chunks.  The model
 repeats the kernel's index arithmetic thread by thread (the producer warp's 32
-threads, which store each chunk; and 256 threads, a wider caller) and checks, for every byte misalignment and chunk lengths from 1 byte to a
+threads, which store the chunks as their stages are refilled, and the compute
+warps' 256 threads, which store the last chunks) and checks, for every byte misalignment and chunk lengths from 1 byte to a
 full raw chunk: every destination byte is written exactly once, nothing outside the
 chunk's bytes is written, and every staged read stays inside the stage."""
 import pytest
