@@ -551,6 +551,11 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
     }
     mbar_fence_init();
   }
+  // the producer's first ticket, taken while the barriers are set up (the
+  // counter was reset by the previous launch's last CTA)
+  long long first_ticket = NO_CHUNK;
+  if (warp == ENC_CW && lane == 0)
+    first_ticket = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long*>(&a.ws[WS_TICKET]), 1ull));
   __syncthreads();
 
   EncSource<BATCH> src = [&]() {
@@ -600,7 +605,7 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
         break;
       }
       long long t = NO_CHUNK;
-      if (lane == 0 && more) t = static_cast<long long>(atomicAdd(tick, 1ull));
+      if (lane == 0 && more) t = seq == 0 ? first_ticket : static_cast<long long>(atomicAdd(tick, 1ull));
       t = __shfl_sync(0xffffffffu, t, 0);
       uint8_t* const stg = stage0 + s * STAGE_BYTES;
       EncMeta& me = m.meta[s];
