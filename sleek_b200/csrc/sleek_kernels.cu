@@ -590,7 +590,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
       __syncwarp();
       return true;
     };
-    int last_seq = 0;
     unsigned issued = 0;      // stages whose last use was a TMA copy (lane 0's view)
     unsigned issued_par = 0;  // parity of that use
     bool more = true;
@@ -653,7 +652,6 @@ __global__ void __launch_bounds__(S::NT, S::MINB) k_encode(const typename std::c
           mbar_arrive(&m.full[s]);
         }
       }
-      last_seq = seq;
       if (!more) break;
     }
     // (the chunks still in stages, the last ENC_STAGES - 1, are stored by the
